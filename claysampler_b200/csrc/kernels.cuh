@@ -1,0 +1,96 @@
+// Device records and kernel launchers shared by the renderer's host code.
+#pragma once
+
+#include "../../include/claysampler_b200.h"
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cs {
+
+constexpr int kTaps = 48;               // render.cu:3
+constexpr int kPhases = 2048;           // render.cu:4
+constexpr int kTileFrames = 256;       // frames per mix tile (one voice list each)
+constexpr int kBlockFrames = CS_TAIL_BLOCK_FRAMES;
+constexpr int kTilesPerBlock = kBlockFrames / kTileFrames;
+
+// A mix tile: kTileFrames frames of one job with the spans that overlap it
+// (the reference's Tile, src/cuda/render_types.h:70-74).
+struct MixTile {
+    int first, count;                   // range in the voice index list
+};
+
+struct JobInfo {
+    uint64_t offset;                    // first frame of the job in the batch mix
+    int frames, musicEnd, limit, fade;
+    int blockFirst, windowFirst, tileFirst;
+    int tracks[4];                      // point offsets bounding CC7, CC11, CC10
+};
+
+// Recurrence state of one voice chain carried across segments
+// (the reference's VoiceState, src/cuda/render_types.h:22-28).
+struct ChainState {
+    double position, step;
+    int pitchSpan, previousLoopEnd, previousLoopStart;
+    int pitchInitialized, filterInitialized;
+    int pad;
+    float z1[CS_FILTER_SLOTS][3][2], z2[CS_FILTER_SLOTS][3][2];
+    float coefficients[CS_FILTER_SLOTS][5];
+};
+
+struct StereoStats { double power; float peak; };
+struct MonoStats { double power; int peak; };
+
+struct TailConfig {                     // src/cuda/render_types.h:100-103
+    int window, quietFrames, padding, fade;
+    double relative, floor, ceiling;
+};
+
+// Everything one synthesis pass reads, as device pointers.
+struct BatchView {
+    const float* bank;
+    const float* sinc;                  // phase-major [2049][48]
+    const cs_voice_span* voices;
+    const cs_control_point* points;
+    const cs_voice_modulation* modulation;
+    const JobInfo* jobs;
+    const MixTile* tiles;
+    const int* indices;
+    const int* blockJob;                // job of each 1024-frame block
+    const int* windowJob;               // job of each tail window
+    ChainState* states;
+    float* filtered;
+    double* phase;
+    void* mix;                          // float2 (natural) or short2
+    int jobCount;
+};
+
+struct SegmentView {
+    int first, end;                     // job-local frame range, 1024-aligned
+    const uint64_t* scratchOffset;      // per voice: float offset into `filtered`
+    const uint64_t* phaseOffset;        // per voice: offset into `phase`
+    const int* chains;                  // heads of chains active in this segment
+    int chainCount;
+    const int* pitchChains;
+    int pitchCount;
+    const int* blocks;                  // mix blocks in this segment
+    int blockCount;
+};
+
+struct FinishView {
+    StereoStats* stereo;
+    MonoStats* windows;
+    short* mono;
+    short* packed;
+    cs_tail_result* results;
+    int blockCount, windowCount;
+};
+
+void buildSincTable(float* phaseMajor);   // host: 2049 x 48 floats
+
+void launchPitch(const BatchView& b, const SegmentView& s, cudaStream_t stream);
+void launchChains(const BatchView& b, const SegmentView& s, cudaStream_t stream);
+void launchMix(const BatchView& b, const SegmentView& s, bool natural, StereoStats* stats, cudaStream_t stream);
+int launchFinish(const BatchView& b, const FinishView& f, bool natural, bool quality, const TailConfig& tail,
+                 cudaStream_t stream);
+
+} // namespace cs

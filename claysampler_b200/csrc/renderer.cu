@@ -1,0 +1,766 @@
+// Host orchestration and C ABI of the B200 renderer.
+//
+// A batch of plans becomes one device arena holding the spans, control points,
+// modulation bindings, per-job records, mix tiles, the float mix and the finishing
+// buffers.  Voice chains that need filter or pitch storage write it to a scratch
+// region; when that storage exceeds the scratch budget the job timeline is cut into
+// 1024-frame-aligned segments and chain state (filter history, coefficient
+// smoothing, pitch phase) carries across them in ChainState, as the reference's
+// segmented synthesis does (src/cuda/renderer.cpp:864-932, render.cu:228-265,345-446).
+#include "kernels.cuh"
+#include "plan_blob.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace cs {
+namespace {
+
+thread_local std::string lastError;
+
+struct CudaError : std::runtime_error {
+    cudaError_t code;
+    CudaError(cudaError_t status, const char* what)
+        : std::runtime_error(std::string(what) + ": " + cudaGetErrorString(status)), code(status) {}
+};
+
+void check(cudaError_t status, const char* what)
+{
+    if (status != cudaSuccess)
+        throw CudaError(status, what);
+}
+
+size_t align256(size_t value) { return (value + 255) & ~size_t(255); }
+
+struct Layout {
+    size_t bytes = 0;
+    size_t add(size_t size)
+    {
+        const size_t offset = align256(bytes);
+        bytes = offset + size;
+        return offset;
+    }
+};
+
+// The reference's BatchIndex::append (src/cuda/renderer.cpp:390-460) restated for
+// this renderer's layout: 256-frame tiles with span-ordered voice lists, rebased
+// control and modulation offsets, and voice chains linked by nextFilteredSpan.
+struct HostBatch {
+    std::vector<cs_voice_span> voices;
+    std::vector<cs_control_point> points;
+    std::vector<cs_voice_modulation> modulation;
+    std::vector<JobInfo> jobs;
+    std::vector<MixTile> tiles;
+    std::vector<int> indices, blockJob, windowJob, chainHeads, pitchHeads;
+    size_t frames = 0;
+    int blocks = 0, windows = 0, lastFrame = 0;
+
+    void append(const cs_plan& plan, int window, bool natural)
+    {
+        if (plan.track_count < 3)
+            throw std::runtime_error("a plan needs its CC7, CC11 and CC10 tracks");
+        const int tileCount = (plan.frames + kTileFrames - 1) / kTileFrames;
+        const int blockCount = (plan.frames + kBlockFrames - 1) / kBlockFrames;
+        const int windowCount = natural ? (plan.frames + window - 1) / window : 0;
+        JobInfo job{};
+        job.offset = frames;
+        job.frames = plan.frames;
+        job.musicEnd = plan.music_end;
+        job.limit = plan.limit;
+        job.fade = plan.fade_frames;
+        job.blockFirst = blocks;
+        job.windowFirst = windows;
+        job.tileFirst = int(tiles.size());
+        std::vector<int> pointOffsets(size_t(plan.track_count) + 1);
+        pointOffsets[0] = int(points.size());
+        for (int i = 0; i < plan.track_count; ++i) {
+            points.insert(points.end(), plan.points + plan.track_offsets[i], plan.points + plan.track_offsets[i + 1]);
+            pointOffsets[size_t(i) + 1] = int(points.size());
+        }
+        for (int i = 0; i < 4; ++i)
+            job.tracks[i] = pointOffsets[size_t(i)];
+        const int modulationBase = int(modulation.size());
+        for (int m = 0; m < plan.modulation_count; ++m) {
+            cs_voice_modulation binding = plan.modulation[m];
+            if (binding.first >= 0) {
+                binding.last = pointOffsets[size_t(binding.first) + 1];
+                binding.first = pointOffsets[size_t(binding.first)];
+            }
+            if (binding.shapeFirst >= 0) {
+                binding.shapeLast = pointOffsets[size_t(binding.shapeFirst) + 1];
+                binding.shapeFirst = pointOffsets[size_t(binding.shapeFirst)];
+            }
+            modulation.push_back(binding);
+        }
+        // Voice lists per tile via a difference array over tile indices.
+        std::vector<int> counts(size_t(tileCount) + 1, 0);
+        for (int s = 0; s < plan.span_count; ++s) {
+            const auto& span = plan.spans[s];
+            if (span.begin < 0 || span.end > plan.frames || span.begin >= span.end)
+                throw std::runtime_error("span outside its job's frames");
+            ++counts[size_t(span.begin / kTileFrames)];
+            --counts[size_t((span.end - 1) / kTileFrames + 1)];
+        }
+        std::partial_sum(counts.begin(), counts.end(), counts.begin());
+        std::vector<int> cursor(static_cast<size_t>(tileCount), 0);
+        int indexCount = int(indices.size());
+        for (int t = 0; t < tileCount; ++t) {
+            tiles.push_back({indexCount, counts[size_t(t)]});
+            cursor[size_t(t)] = indexCount;
+            indexCount += counts[size_t(t)];
+        }
+        indices.resize(size_t(indexCount));
+        std::vector<int> chainTail(size_t(plan.filter_tracks), -1);
+        for (int s = 0; s < plan.span_count; ++s) {
+            cs_voice_span voice = plan.spans[s];
+            const int index = int(voices.size());
+            for (int t = voice.begin / kTileFrames; t <= (voice.end - 1) / kTileFrames; ++t)
+                indices[size_t(cursor[size_t(t)]++)] = index;
+            voice.firstModulation += modulationBase;
+            if (voice.filterTrack >= 0) {
+                if (voice.filterTrack >= plan.filter_tracks)
+                    throw std::runtime_error("span filter track outside the plan's filter_tracks");
+                int& tail = chainTail[size_t(voice.filterTrack)];
+                if (tail < 0) {
+                    chainHeads.push_back(index);
+                    if (voice.variablePitch)
+                        pitchHeads.push_back(index);
+                } else {
+                    voices[size_t(tail)].nextFilteredSpan = index;
+                }
+                tail = index;
+                voice.nextFilteredSpan = -1;
+                for (int i = 0; i < 4; ++i)
+                    voice.filterControls[i] = pointOffsets[size_t(i)];
+            }
+            voices.push_back(voice);
+        }
+        for (int b = 0; b < blockCount; ++b)
+            blockJob.push_back(int(jobs.size()));
+        for (int w = 0; w < windowCount; ++w)
+            windowJob.push_back(int(jobs.size()));
+        jobs.push_back(job);
+        frames += size_t(plan.frames);
+        blocks += blockCount;
+        windows += windowCount;
+        lastFrame = std::max(lastFrame, plan.frames);
+    }
+};
+
+struct SegmentPlan {
+    int first, end;
+    size_t scratchFloats, phaseFrames;
+    size_t chainFirst, chainCount, pitchFirst, pitchCount, blockFirst, blockCount;
+};
+
+// Host side of a staged batch: segment boundaries and the per-segment arrays.
+struct SegmentTables {
+    std::vector<SegmentPlan> segments;
+    std::vector<uint64_t> scratchOffset, phaseOffset;   // segments x voices
+    std::vector<int> chains, pitch, blocks;
+    size_t scratchBytes = 0;
+};
+
+size_t scratchBytesOf(size_t floats, size_t phases) { return align256(floats * sizeof(float)) + phases * sizeof(double); }
+
+// Cuts [0, lastFrame) at 1024-frame boundaries so that each segment's chain
+// storage fits `budget` (one block per segment at least).
+SegmentTables planSegments(const HostBatch& batch, size_t budget)
+{
+    SegmentTables t;
+    const int lastFrame = batch.lastFrame;
+    const int blocks = (lastFrame + kBlockFrames - 1) / kBlockFrames;
+    // Per-block storage demand of every chain span, via a difference array.
+    std::vector<long long> floatsPerBlock(size_t(blocks) + 1, 0), phasesPerBlock(size_t(blocks) + 1, 0);
+    for (const auto& v : batch.voices) {
+        if (v.filterTrack < 0)
+            continue;
+        for (int b = v.begin / kBlockFrames; b <= (v.end - 1) / kBlockFrames; ++b) {
+            const int lo = std::max(v.begin, b * kBlockFrames), hi = std::min(v.end, (b + 1) * kBlockFrames);
+            floatsPerBlock[size_t(b)] += (long long)(hi - lo) * v.channels;
+            if (v.variablePitch)
+                phasesPerBlock[size_t(b)] += hi - lo;
+        }
+    }
+    std::vector<std::pair<int, int>> ranges;
+    for (int b = 0; b < blocks;) {
+        size_t floats = 0, phases = 0;
+        int e = b;
+        while (e < blocks) {
+            const size_t nf = floats + size_t(floatsPerBlock[size_t(e)]);
+            const size_t np = phases + size_t(phasesPerBlock[size_t(e)]);
+            if (e > b && scratchBytesOf(nf, np) > budget)
+                break;
+            floats = nf;
+            phases = np;
+            ++e;
+        }
+        ranges.emplace_back(b * kBlockFrames, std::min(lastFrame, e * kBlockFrames));
+        b = e;
+    }
+    if (ranges.empty())
+        ranges.emplace_back(0, 0);
+    const size_t voiceCount = batch.voices.size();
+    t.scratchOffset.assign(voiceCount * ranges.size(), 0);
+    t.phaseOffset.assign(voiceCount * ranges.size(), 0);
+    for (size_t si = 0; si < ranges.size(); ++si) {
+        SegmentPlan seg{};
+        seg.first = ranges[si].first;
+        seg.end = ranges[si].second;
+        size_t floats = 0, phases = 0;
+        for (size_t v = 0; v < voiceCount; ++v) {
+            const auto& voice = batch.voices[v];
+            if (voice.filterTrack < 0)
+                continue;
+            const int frames = std::max(0, std::min(voice.end, seg.end) - std::max(voice.begin, seg.first));
+            t.scratchOffset[si * voiceCount + v] = floats;
+            t.phaseOffset[si * voiceCount + v] = phases;
+            floats += size_t(frames) * size_t(voice.channels);
+            if (voice.variablePitch)
+                phases += size_t(frames);
+        }
+        seg.scratchFloats = floats;
+        seg.phaseFrames = phases;
+        t.scratchBytes = std::max(t.scratchBytes, scratchBytesOf(floats, phases));
+        const auto active = [&](int head) {
+            for (int span = head; span >= 0; span = batch.voices[size_t(span)].nextFilteredSpan) {
+                const auto& v = batch.voices[size_t(span)];
+                if (v.begin >= seg.end)
+                    break;
+                if (v.end > seg.first)
+                    return true;
+            }
+            return false;
+        };
+        seg.chainFirst = t.chains.size();
+        for (int head : batch.chainHeads)
+            if (active(head))
+                t.chains.push_back(head);
+        seg.chainCount = t.chains.size() - seg.chainFirst;
+        seg.pitchFirst = t.pitch.size();
+        for (int head : batch.pitchHeads)
+            if (active(head))
+                t.pitch.push_back(head);
+        seg.pitchCount = t.pitch.size() - seg.pitchFirst;
+        seg.blockFirst = t.blocks.size();
+        for (const auto& job : batch.jobs) {
+            const int jobBlocks = (job.frames + kBlockFrames - 1) / kBlockFrames;
+            for (int b = seg.first / kBlockFrames; b < std::min(jobBlocks, (seg.end + kBlockFrames - 1) / kBlockFrames); ++b)
+                t.blocks.push_back(job.blockFirst + b);
+        }
+        seg.blockCount = t.blocks.size() - seg.blockFirst;
+        t.segments.push_back(seg);
+    }
+    return t;
+}
+
+} // namespace
+} // namespace cs
+
+struct cs_prepared {
+    cs_renderer* owner = nullptr;
+    cs::HostBatch batch;
+    cs::SegmentTables tables;
+    void* arena = nullptr;
+    size_t arenaBytes = 0;
+    cs::BatchView view{};
+    std::vector<cs::SegmentView> segments;
+    cs::FinishView finish{};
+    cs::StereoStats* stereo = nullptr;
+    size_t stateBytes = 0, resultBytes = 0, mixBytes = 0;
+    bool natural = true;
+    int launches = 0;
+    cudaEvent_t begin = nullptr, end = nullptr;
+    std::vector<cs_tail_result> results;
+    bool ran = false;
+};
+
+struct cs_renderer {
+    int device = 0;
+    bool natural = true;
+    cs_audio_config audio{};
+    int groupMinimum = 0;
+    size_t waitingLimit = 0, batchJobs = 64;
+    cs::TailConfig tail{};
+    std::string name;
+    cudaStream_t stream = nullptr;
+    float* sinc = nullptr;
+    float* bank = nullptr;
+    size_t bankCapacity = 0, uploaded = 0;
+    size_t scratchLimit = 0;            // 0: derive from free memory
+    size_t peak = 0, waiting = 0, peakWaiting = 0, spilled = 0, downloaded = 0, cacheBudget = 0;
+    size_t live = 0;                    // bytes of prepared batches alive
+    void* hostPcm = nullptr;
+    size_t hostPcmCapacity = 0;
+
+    void record(size_t extra = 0)
+    {
+        const size_t sincBytes = size_t(cs::kTaps) * (cs::kPhases + 1) * sizeof(float);
+        peak = std::max(peak, sincBytes + bankCapacity * sizeof(float) + live + extra);
+    }
+};
+
+namespace cs {
+namespace {
+
+size_t defaultScratchBudget()
+{
+    size_t freeBytes = 0, total = 0;
+    check(cudaMemGetInfo(&freeBytes, &total), "CUDA free memory");
+    // The reference bounds a batch by min(3/4 available, total / 4); its chain
+    // storage shares that budget with the mix and finishing buffers.
+    return std::max<size_t>(size_t(1) << 20, std::min(freeBytes / 2, total / 4));
+}
+
+cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count)
+{
+    check(cudaSetDevice(r.device), "CUDA device");
+    auto p = std::make_unique<cs_prepared>();
+    p->owner = &r;
+    p->natural = r.natural;
+    HostBatch& batch = p->batch;
+    for (size_t i = 0; i < count; ++i)
+        batch.append(plans[i], r.tail.window, r.natural);
+    p->tables = planSegments(batch, r.scratchLimit ? r.scratchLimit : defaultScratchBudget());
+    const SegmentTables& t = p->tables;
+    const size_t jobs = batch.jobs.size();
+    const size_t frameBytes = r.natural ? sizeof(float2) : sizeof(short2);
+    const int channels = r.natural ? 1 : 2;
+
+    Layout layout;
+    const auto section = [&](size_t bytes) { return layout.add(std::max<size_t>(bytes, 1)); };
+    const size_t oVoices = section(batch.voices.size() * sizeof(cs_voice_span));
+    const size_t oPoints = section(batch.points.size() * sizeof(cs_control_point));
+    const size_t oMods = section(batch.modulation.size() * sizeof(cs_voice_modulation));
+    const size_t oJobs = section(jobs * sizeof(JobInfo));
+    const size_t oTiles = section(batch.tiles.size() * sizeof(MixTile));
+    const size_t oIndices = section(batch.indices.size() * sizeof(int));
+    const size_t oBlockJob = section(batch.blockJob.size() * sizeof(int));
+    const size_t oWindowJob = section(batch.windowJob.size() * sizeof(int));
+    const size_t oScratchOff = section(t.scratchOffset.size() * sizeof(uint64_t));
+    const size_t oPhaseOff = section(t.phaseOffset.size() * sizeof(uint64_t));
+    const size_t oChains = section(t.chains.size() * sizeof(int));
+    const size_t oPitch = section(t.pitch.size() * sizeof(int));
+    const size_t oBlocks = section(t.blocks.size() * sizeof(int));
+    const size_t uploadEnd = layout.bytes;
+    p->stateBytes = batch.voices.size() * sizeof(ChainState);
+    const size_t oStates = section(p->stateBytes);
+    p->resultBytes = jobs * sizeof(cs_tail_result);
+    const size_t oResults = section(p->resultBytes);
+    p->mixBytes = batch.frames * frameBytes;
+    const size_t oMix = section(p->mixBytes);
+    const size_t oStereo = section(size_t(batch.blocks) * sizeof(StereoStats));
+    const size_t oWindows = section(size_t(batch.windows) * sizeof(MonoStats));
+    const size_t oMono = section(r.natural ? batch.frames * sizeof(short) : 0);
+    const size_t oPacked = section(batch.frames * size_t(channels) * sizeof(short));
+    const size_t oScratch = section(t.scratchBytes);
+    p->arenaBytes = layout.bytes;
+
+    cudaError_t status = cudaMalloc(&p->arena, p->arenaBytes);
+    if (status != cudaSuccess) {
+        cudaGetLastError();
+        p->arena = nullptr;
+        throw CudaError(status, "CUDA batch arena allocation");
+    }
+    r.live += p->arenaBytes;
+    r.record();
+    auto* base = static_cast<unsigned char*>(p->arena);
+    std::vector<unsigned char> staging(uploadEnd, 0);
+    const auto stage = [&](size_t offset, const auto& items) {
+        if (!items.empty())
+            std::memcpy(staging.data() + offset, items.data(), items.size() * sizeof(items.front()));
+    };
+    stage(oVoices, batch.voices);
+    stage(oPoints, batch.points);
+    stage(oMods, batch.modulation);
+    stage(oJobs, batch.jobs);
+    stage(oTiles, batch.tiles);
+    stage(oIndices, batch.indices);
+    stage(oBlockJob, batch.blockJob);
+    stage(oWindowJob, batch.windowJob);
+    stage(oScratchOff, t.scratchOffset);
+    stage(oPhaseOff, t.phaseOffset);
+    stage(oChains, t.chains);
+    stage(oPitch, t.pitch);
+    stage(oBlocks, t.blocks);
+    check(cudaMemcpyAsync(base, staging.data(), uploadEnd, cudaMemcpyHostToDevice, r.stream), "CUDA batch upload");
+    check(cudaStreamSynchronize(r.stream), "CUDA batch upload");
+
+    BatchView& v = p->view;
+    v.bank = r.bank;
+    v.sinc = r.sinc;
+    v.voices = reinterpret_cast<const cs_voice_span*>(base + oVoices);
+    v.points = reinterpret_cast<const cs_control_point*>(base + oPoints);
+    v.modulation = reinterpret_cast<const cs_voice_modulation*>(base + oMods);
+    v.jobs = reinterpret_cast<const JobInfo*>(base + oJobs);
+    v.tiles = reinterpret_cast<const MixTile*>(base + oTiles);
+    v.indices = reinterpret_cast<const int*>(base + oIndices);
+    v.blockJob = reinterpret_cast<const int*>(base + oBlockJob);
+    v.windowJob = reinterpret_cast<const int*>(base + oWindowJob);
+    v.states = reinterpret_cast<ChainState*>(base + oStates);
+    v.filtered = reinterpret_cast<float*>(base + oScratch);
+    v.mix = base + oMix;
+    v.jobCount = int(jobs);
+    const size_t voiceCount = batch.voices.size();
+    for (const auto& seg : t.segments) {
+        SegmentView s{};
+        const size_t si = size_t(&seg - t.segments.data());
+        s.first = seg.first;
+        s.end = seg.end;
+        s.scratchOffset = reinterpret_cast<const uint64_t*>(base + oScratchOff) + si * voiceCount;
+        s.phaseOffset = reinterpret_cast<const uint64_t*>(base + oPhaseOff) + si * voiceCount;
+        s.chains = reinterpret_cast<const int*>(base + oChains) + seg.chainFirst;
+        s.chainCount = int(seg.chainCount);
+        s.pitchChains = reinterpret_cast<const int*>(base + oPitch) + seg.pitchFirst;
+        s.pitchCount = int(seg.pitchCount);
+        s.blocks = reinterpret_cast<const int*>(base + oBlocks) + seg.blockFirst;
+        s.blockCount = int(seg.blockCount);
+        p->segments.push_back(s);
+    }
+    // Pitch phases follow the filtered floats of the same segment.
+    v.phase = reinterpret_cast<double*>(base + oScratch);
+    FinishView& f = p->finish;
+    f.stereo = reinterpret_cast<StereoStats*>(base + oStereo);
+    f.windows = reinterpret_cast<MonoStats*>(base + oWindows);
+    f.mono = reinterpret_cast<short*>(base + oMono);
+    f.packed = reinterpret_cast<short*>(base + oPacked);
+    f.results = reinterpret_cast<cs_tail_result*>(base + oResults);
+    f.blockCount = batch.blocks;
+    f.windowCount = batch.windows;
+    p->stereo = f.stereo;
+    check(cudaEventCreate(&p->begin), "CUDA timing event");
+    check(cudaEventCreate(&p->end), "CUDA timing event");
+    return p.release();
+}
+
+void run(cs_renderer& r, cs_prepared& p, cudaStream_t stream)
+{
+    check(cudaSetDevice(r.device), "CUDA device");
+    if (!stream)
+        stream = r.stream;
+    p.view.bank = r.bank;
+    p.view.sinc = r.sinc;
+    int launches = 0;
+    check(cudaEventRecord(p.begin, stream), "CUDA timing record");
+    check(cudaMemsetAsync(p.view.states, 0, std::max<size_t>(p.stateBytes, 1), stream), "CUDA state reset");
+    check(cudaMemsetAsync(p.finish.results, 0, std::max<size_t>(p.resultBytes, 1), stream), "CUDA result reset");
+    for (size_t i = 0; i < p.segments.size(); ++i) {
+        BatchView view = p.view;
+        const SegmentPlan& plan = p.tables.segments[i];
+        view.phase = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(view.filtered) +
+                                               align256(plan.scratchFloats * sizeof(float)));
+        const SegmentView& s = p.segments[i];
+        launchPitch(view, s, stream);
+        launchChains(view, s, stream);
+        launchMix(view, s, r.natural, p.stereo, stream);
+        launches += (s.pitchCount > 0) + (s.chainCount > 0) + (s.blockCount > 0);
+    }
+    check(cudaGetLastError(), "CUDA synthesis launch");
+    launches += launchFinish(p.view, p.finish, r.natural, r.audio.enabled != 0, r.tail, stream);
+    check(cudaGetLastError(), "CUDA finishing launch");
+    check(cudaEventRecord(p.end, stream), "CUDA timing record");
+    p.launches = launches;
+    p.ran = true;
+}
+
+// Synchronises and reads the results; returns the packed PCM sample count.
+size_t collectResults(cs_renderer& r, cs_prepared& p)
+{
+    check(cudaEventSynchronize(p.end), "CUDA render completion");
+    p.results.resize(p.batch.jobs.size());
+    check(cudaMemcpy(p.results.data(), p.finish.results, p.resultBytes, cudaMemcpyDeviceToHost),
+          "CUDA render metadata download");
+    if (p.results.empty())
+        return 0;
+    const auto& last = p.results.back();
+    return size_t(last.offset + uint64_t(last.dataFrames)) * (r.natural ? 1 : 2);
+}
+
+void checkPlans(const cs_plan* plans, size_t count)
+{
+    if (count && !plans)
+        throw std::runtime_error("null plan array");
+    for (size_t i = 0; i < count; ++i) {
+        const cs_plan& p = plans[i];
+        if (p.frames <= 0 || (p.span_count && !p.spans) || p.track_count < 3 || !p.track_offsets ||
+            (p.modulation_count && !p.modulation))
+            throw std::runtime_error("invalid plan " + std::to_string(i));
+    }
+}
+
+template <class F>
+int guarded(F&& body)
+{
+    try {
+        body();
+        return 0;
+    } catch (const std::exception& e) {
+        lastError = e.what();
+        return 1;
+    }
+}
+
+} // namespace
+} // namespace cs
+
+extern "C" {
+
+const char* cs_last_error(void) { return cs::lastError.c_str(); }
+
+int cs_renderer_create(int device, int natural, const cs_audio_config* audio, int group_minimum,
+                       size_t waiting_limit, size_t batch_jobs, cs_renderer** out)
+{
+    return cs::guarded([&] {
+        if (!out)
+            throw std::runtime_error("null output handle");
+        *out = nullptr;
+        auto r = std::make_unique<cs_renderer>();
+        r->device = device;
+        r->natural = natural != 0;
+        if (audio) {
+            r->audio = *audio;
+        } else {
+            r->audio.rate = 44100;
+            r->audio.window = 2205;
+        }
+        if (r->audio.rate <= 0 || r->audio.window <= 0)
+            throw std::runtime_error("audio config needs a positive rate and window");
+        r->groupMinimum = group_minimum;
+        r->waitingLimit = waiting_limit;
+        r->batchJobs = std::max<size_t>(1, batch_jobs);
+        const int rate = r->audio.rate;
+        // TailConfig of the reference renderer (src/cuda/renderer.cpp:492-494).
+        r->tail = {r->audio.window, 2 * rate, int(std::nearbyint(rate / 4.)), int(std::nearbyint(rate / 10.)),
+                   std::pow(10., -1.5), 32768 * std::pow(10., -3.9), 32768 * std::pow(10., -3.)};
+        cs::check(cudaSetDevice(device), "CUDA device");
+        cudaDeviceProp prop{};
+        cs::check(cudaGetDeviceProperties(&prop, device), "CUDA device properties");
+        if (prop.major < 10)
+            throw std::runtime_error(std::string("claysampler_b200 needs an sm_100 GPU, found ") + prop.name);
+        r->name = prop.name;
+        cs::check(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking), "CUDA stream");
+        std::vector<float> table(size_t(cs::kTaps) * (cs::kPhases + 1));
+        cs::buildSincTable(table.data());
+        cs::check(cudaMalloc(&r->sinc, table.size() * sizeof(float)), "CUDA sinc table");
+        cs::check(cudaMemcpy(r->sinc, table.data(), table.size() * sizeof(float), cudaMemcpyHostToDevice),
+                  "CUDA sinc upload");
+        size_t freeBytes = 0, total = 0;
+        cs::check(cudaMemGetInfo(&freeBytes, &total), "CUDA sample cache budget");
+        r->cacheBudget = std::min(freeBytes - freeBytes / 3, total / 2);
+        r->record();
+        *out = r.release();
+    });
+}
+
+void cs_renderer_destroy(cs_renderer* r)
+{
+    if (!r)
+        return;
+    cudaSetDevice(r->device);
+    if (r->stream) cudaStreamSynchronize(r->stream);
+    cudaFree(r->sinc);
+    cudaFree(r->bank);
+    if (r->hostPcm) cudaFreeHost(r->hostPcm);
+    if (r->stream) cudaStreamDestroy(r->stream);
+    delete r;
+}
+
+int cs_upload_samples(cs_renderer* r, const float* pcm, size_t floats, int fresh)
+{
+    return cs::guarded([&] {
+        if (!r)
+            throw std::runtime_error("null renderer");
+        cs::check(cudaSetDevice(r->device), "CUDA device");
+        if (fresh)
+            r->uploaded = 0;
+        if (floats <= r->uploaded && r->bank)
+            return;
+        if (floats > r->bankCapacity) {
+            // Grow with slack and keep what was uploaded (src/cuda/renderer.cpp:564-586).
+            const size_t capacity = floats + std::min(floats / 2, size_t(32) << 20);
+            float* grown = nullptr;
+            cs::check(cudaMalloc(&grown, capacity * sizeof(float)), "CUDA sample bank allocation");
+            if (r->uploaded)
+                cs::check(cudaMemcpy(grown, r->bank, r->uploaded * sizeof(float), cudaMemcpyDeviceToDevice),
+                          "CUDA sample bank growth");
+            cudaFree(r->bank);
+            r->bank = grown;
+            r->bankCapacity = capacity;
+        }
+        if (floats > r->uploaded)
+            cs::check(cudaMemcpy(r->bank + r->uploaded, pcm + r->uploaded, (floats - r->uploaded) * sizeof(float),
+                                 cudaMemcpyHostToDevice), "CUDA sample upload");
+        r->uploaded = floats;
+        r->record();
+    });
+}
+
+int cs_prepare(cs_renderer* r, const cs_plan* plans, size_t count, cs_prepared** out)
+{
+    return cs::guarded([&] {
+        if (!r || !out)
+            throw std::runtime_error("null renderer or output handle");
+        cs::checkPlans(plans, count);
+        *out = cs::prepare(*r, plans, count);
+    });
+}
+
+int cs_run(cs_renderer* r, cs_prepared* p, void* stream)
+{
+    return cs::guarded([&] {
+        if (!r || !p)
+            throw std::runtime_error("null renderer or batch");
+        if (!r->bank && !p->batch.voices.empty())
+            throw std::runtime_error("no sample bank uploaded");
+        cs::run(*r, *p, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int cs_collect(cs_renderer* r, cs_prepared* p, int16_t* pcm, size_t capacity, size_t* samples,
+               cs_tail_result* results)
+{
+    return cs::guarded([&] {
+        if (!r || !p || !p->ran)
+            throw std::runtime_error("batch has not been run");
+        const size_t count = cs::collectResults(*r, *p);
+        if (samples)
+            *samples = count;
+        if (results && !p->results.empty())
+            std::memcpy(results, p->results.data(), p->results.size() * sizeof(cs_tail_result));
+        if (pcm) {
+            if (capacity < count)
+                throw std::runtime_error("PCM buffer too small");
+            if (count)
+                cs::check(cudaMemcpy(pcm, p->finish.packed, count * sizeof(int16_t), cudaMemcpyDeviceToHost),
+                          "CUDA PCM download");
+            r->downloaded += count * sizeof(int16_t);
+        }
+    });
+}
+
+int cs_copy_mix(cs_renderer* r, cs_prepared* p, void* host, size_t bytes)
+{
+    return cs::guarded([&] {
+        if (!r || !p || !p->ran)
+            throw std::runtime_error("batch has not been run");
+        if (bytes < p->mixBytes)
+            throw std::runtime_error("mix buffer too small");
+        cs::check(cudaEventSynchronize(p->end), "CUDA render completion");
+        cs::check(cudaMemcpy(host, p->view.mix, p->mixBytes, cudaMemcpyDeviceToHost), "CUDA mix download");
+    });
+}
+
+size_t cs_prepared_frames(const cs_prepared* p) { return p ? p->batch.frames : 0; }
+int cs_prepared_launches(const cs_prepared* p) { return p ? p->launches : 0; }
+
+void cs_prepared_destroy(cs_prepared* p)
+{
+    if (!p)
+        return;
+    if (p->end) cudaEventSynchronize(p->end);
+    if (p->begin) cudaEventDestroy(p->begin);
+    if (p->end) cudaEventDestroy(p->end);
+    if (p->arena) {
+        cudaFree(p->arena);
+        if (p->owner)
+            p->owner->live -= p->arenaBytes;
+    }
+    delete p;
+}
+
+int cs_render_window(cs_renderer* r, const cs_plan* plans, size_t count, cs_publish_fn publish,
+                     cs_refill_fn refill, void* user)
+{
+    return cs::guarded([&] {
+        if (!r || !publish)
+            throw std::runtime_error("null renderer or publish callback");
+        std::vector<cs_plan> queue(plans, plans + count);
+        cs::checkPlans(plans, count);
+        size_t first = 0;
+        std::vector<int16_t> pcm;
+        for (;;) {
+            if (first == queue.size()) {
+                const cs_plan* more = nullptr;
+                size_t moreCount = 0;
+                if (!refill || !refill(user, 1, &more, &moreCount) || !moreCount)
+                    break;
+                cs::checkPlans(more, moreCount);
+                queue.insert(queue.end(), more, more + moreCount);
+            }
+            size_t jobs = std::min(r->batchJobs, queue.size() - first);
+            cs_prepared* prepared = nullptr;
+            for (;;) {
+                try {
+                    prepared = cs::prepare(*r, queue.data() + first, jobs);
+                    break;
+                } catch (const cs::CudaError& e) {
+                    if (e.code != cudaErrorMemoryAllocation)
+                        throw;
+                    // Allocation recovery: retry with half the jobs, then reject the
+                    // single job (src/cuda/renderer.cpp:947-992).
+                    if (jobs > 1) {
+                        jobs /= 2;
+                        continue;
+                    }
+                    break;
+                }
+            }
+            if (!prepared) {
+                cs_batch rejected{};
+                rejected.failed_scratch_bytes = 1;
+                publish(user, &rejected, first);
+                first += 1;
+                continue;
+            }
+            std::unique_ptr<cs_prepared, void (*)(cs_prepared*)> guard(prepared, cs_prepared_destroy);
+            cs::run(*r, *prepared, nullptr);
+            const size_t samples = cs::collectResults(*r, *prepared);
+            pcm.resize(samples);
+            if (samples)
+                cs::check(cudaMemcpy(pcm.data(), prepared->finish.packed, samples * sizeof(int16_t),
+                                     cudaMemcpyDeviceToHost), "CUDA PCM download");
+            r->downloaded += samples * sizeof(int16_t);
+            float ms = 0;
+            cs::check(cudaEventElapsedTime(&ms, prepared->begin, prepared->end), "CUDA kernel timing");
+            cs_batch batch{};
+            batch.pcm = pcm.data();
+            batch.pcm_samples = samples;
+            batch.results = prepared->results.data();
+            batch.result_count = prepared->results.size();
+            batch.kernel_seconds = ms / 1000.0;
+            publish(user, &batch, first);
+            first += jobs;
+        }
+    });
+}
+
+const char* cs_renderer_device(const cs_renderer* r) { return r ? r->name.c_str() : ""; }
+size_t cs_peak_bytes(const cs_renderer* r) { return r ? r->peak : 0; }
+size_t cs_sample_cache_budget(const cs_renderer* r) { return r ? r->cacheBudget : 0; }
+size_t cs_peak_waiting_bytes(const cs_renderer* r) { return r ? r->peakWaiting : 0; }
+size_t cs_spilled_bytes(const cs_renderer* r) { return r ? r->spilled : 0; }
+size_t cs_downloaded_bytes(const cs_renderer* r) { return r ? r->downloaded : 0; }
+
+// Caps the chain-storage bytes of one synthesis segment (0 restores the default
+// derived from free device memory).  No reference counterpart: the reference
+// exercises segmentation with a special build that limits scratch to 64 KiB.
+int cs_renderer_set_scratch_limit(cs_renderer* r, size_t bytes)
+{
+    return cs::guarded([&] {
+        if (!r)
+            throw std::runtime_error("null renderer");
+        r->scratchLimit = bytes;
+    });
+}
+
+size_t cs_prepared_segments(const cs_prepared* p) { return p ? p->tables.segments.size() : 0; }
+
+} // extern "C"

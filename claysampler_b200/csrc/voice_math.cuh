@@ -1,0 +1,361 @@
+// Per-voice, per-frame arithmetic of the render path.  Each function restates the
+// reference's definition (src/cuda/render.cu) operation for operation, because the
+// float bus is checked against the reference within 1e-5 of full scale and PCM16 to
+// one LSB: the build uses --fmad=false so only the explicit fmaf calls fuse, as in
+// the reference compiled for the host.
+#pragma once
+
+#include "kernels.cuh"
+#include <stdint.h>
+
+namespace cs {
+
+constexpr float kQuarterPi = .7853981633974483f;
+
+// Amplitude / filter / pitch envelope value at `frame` (render.cu:6-19).
+template <class Shape>
+__device__ __forceinline__ float envelopeAt(const Shape& e, int frame)
+{
+    if (e.releaseStart >= 0 && frame >= e.releaseStart) {
+        if (frame >= e.fadeStart)
+            return fmaxf(0.f, e.fadeValue - float(frame - e.fadeStart + 1) * e.fadeStep);
+        return e.releaseValue * expf(float(frame - e.releaseStart + 1) * e.releaseRate);
+    }
+    if (frame < e.attackStart) return e.start;
+    if (frame < e.holdStart) return fminf(1.f, e.start + float(frame - e.attackStart + 1) * e.attackStep);
+    if (frame < e.decayStart) return 1.f;
+    if (e.decayRate == 0) return e.sustain;
+    return fmaxf(e.sustain, expf(float(frame - e.decayStart + 1) * e.decayRate));
+}
+
+// Piecewise-linear track value: the last point with point.frame <= frame in
+// [low, high) (render.cu:107-118).
+__device__ __forceinline__ float trackAt(const cs_control_point* __restrict__ points, int low, int high, int frame)
+{
+    while (low + 1 < high) {
+        const int mid = low + (high - low) / 2;
+        if (__ldg(&points[mid].frame) <= frame) low = mid;
+        else high = mid;
+    }
+    const int at = __ldg(&points[low].frame);
+    return fmaf(__ldg(&points[low].step), float(frame - at), __ldg(&points[low].value));
+}
+
+__device__ __forceinline__ float bindingAt(const cs_voice_modulation& m, const cs_control_point* __restrict__ points,
+                                           int frame)
+{
+    float value = m.first < 0 ? m.depth : m.depth * trackAt(points, m.first, m.last, frame);
+    if (m.shapeFirst >= 0)
+        value *= trackAt(points, m.shapeFirst, m.shapeLast, frame);
+    return value;
+}
+
+// CC7 x CC11 job gain (render.cu:189-193); `tracks` holds the job's first four
+// track point offsets.
+__device__ __forceinline__ float jobGainAt(const cs_control_point* __restrict__ points, const int* tracks, int frame)
+{
+    return trackAt(points, tracks[0], tracks[1], frame) * trackAt(points, tracks[1], tracks[2], frame);
+}
+
+// Source frame with zero outside [0, sourceEnd) (render.cu:21-28).
+__device__ __forceinline__ float2 sourceFrame(const float* __restrict__ bank, const cs_voice_span& v, int frame)
+{
+    if (frame < 0 || frame >= v.sourceEnd)
+        return make_float2(0.f, 0.f);
+    const uint64_t index = v.sample + uint64_t(frame) * uint64_t(v.channels);
+    const float left = __ldg(bank + index);
+    return make_float2(left, v.channels == 1 ? left : __ldg(bank + index + 1));
+}
+
+// 48-tap windowed-sinc value at `pos` (render.cu:30-61).  The table is stored
+// phase-major, 48 contiguous weights per phase, so each lane streams its row with
+// 128-bit loads; the tap order of the accumulation is unchanged.
+__device__ __forceinline__ float2 sincAt(const float* __restrict__ bank, const float* __restrict__ sinc,
+                                         const cs_voice_span& v, double pos)
+{
+    const int center = __double2int_rd(pos);
+    if (pos == double(center))
+        return sourceFrame(bank, v, center);
+    const int phase = __double2int_rn((pos - double(center)) * kPhases);
+    const float4* row = reinterpret_cast<const float4*>(sinc + size_t(phase) * kTaps);
+    float x = 0.f, y = 0.f;
+    if (center >= 23 && center < v.sourceEnd - 24) {
+        const float* s = bank + v.sample + uint64_t(center - 23) * uint64_t(v.channels);
+        if (v.channels == 1) {
+            #pragma unroll
+            for (int q = 0; q < kTaps / 4; ++q) {
+                const float4 w = __ldg(row + q);
+                x = fmaf(w.x, __ldg(s + 4 * q + 0), x);
+                x = fmaf(w.y, __ldg(s + 4 * q + 1), x);
+                x = fmaf(w.z, __ldg(s + 4 * q + 2), x);
+                x = fmaf(w.w, __ldg(s + 4 * q + 3), x);
+            }
+            y = x;
+        } else if ((reinterpret_cast<uintptr_t>(s) & 7) == 0) {
+            const float2* s2 = reinterpret_cast<const float2*>(s);
+            #pragma unroll
+            for (int q = 0; q < kTaps / 4; ++q) {
+                const float4 w = __ldg(row + q);
+                const float2 p0 = __ldg(s2 + 4 * q + 0);
+                const float2 p1 = __ldg(s2 + 4 * q + 1);
+                const float2 p2 = __ldg(s2 + 4 * q + 2);
+                const float2 p3 = __ldg(s2 + 4 * q + 3);
+                x = fmaf(w.x, p0.x, x); y = fmaf(w.x, p0.y, y);
+                x = fmaf(w.y, p1.x, x); y = fmaf(w.y, p1.y, y);
+                x = fmaf(w.z, p2.x, x); y = fmaf(w.z, p2.y, y);
+                x = fmaf(w.w, p3.x, x); y = fmaf(w.w, p3.y, y);
+            }
+        } else {
+            // A stereo sample that starts at an odd float offset (after an odd-length
+            // mono sample in the bank) cannot use 8-byte loads.
+            #pragma unroll 4
+            for (int q = 0; q < kTaps / 4; ++q) {
+                const float4 w = __ldg(row + q);
+                const float ws[4] = {w.x, w.y, w.z, w.w};
+                #pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    x = fmaf(ws[k], __ldg(s + 2 * (4 * q + k)), x);
+                    y = fmaf(ws[k], __ldg(s + 2 * (4 * q + k) + 1), y);
+                }
+            }
+        }
+    } else {
+        for (int q = 0; q < kTaps / 4; ++q) {
+            const float4 w = __ldg(row + q);
+            const float ws[4] = {w.x, w.y, w.z, w.w};
+            #pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const float2 s = sourceFrame(bank, v, center - 23 + 4 * q + k);
+                x = fmaf(ws[k], s.x, x);
+                y = fmaf(ws[k], s.y, y);
+            }
+        }
+    }
+    return make_float2(x, y);
+}
+
+// Source value of a voice at output `frame` (render.cu:63-100): position from the
+// span's start (or a precomputed variable-pitch phase), generators, loop wrap and
+// loop crossfade.
+__device__ __forceinline__ float2 voiceSource(const float* __restrict__ bank, const float* __restrict__ sinc,
+                                              const cs_voice_span& v, int frame, double pos)
+{
+    if (pos < 0) {
+        const int elapsed = frame - v.begin;
+        double distance = elapsed;
+        if (v.pitchSlope != 0)
+            distance = expm1(v.pitchSlope * elapsed) / expm1(v.pitchSlope);
+        pos = v.position + distance * v.step;
+    }
+    if (v.generator != CS_GEN_NONE) {
+        if (v.generator == CS_GEN_NOISE) {
+            unsigned bits = v.noiseSeed + unsigned(frame - v.noiseStart);
+            bits = (bits ^ (bits >> 16)) * 0x7feb352du;
+            bits = (bits ^ (bits >> 15)) * 0x846ca68bu;
+            bits ^= bits >> 16;
+            const float value = float(bits >> 8) * (2.f / 16777216.f) - 1.f;
+            return make_float2(value, value);
+        }
+        const float value = v.generator == CS_GEN_SINE
+            ? -sinf(6.28318530717958647692f * float(pos - floor(pos))) : 0.f;
+        return make_float2(value, value);
+    }
+    const int period = v.loopEnd - v.loopFirst;
+    if (v.loopEnd > 0 && pos >= v.loopEnd)
+        pos = v.loopFirst + fmod(pos - v.loopFirst, double(period));
+    if (pos >= v.sourceEnd)
+        return make_float2(0.f, 0.f);
+    float2 sample = sincAt(bank, sinc, v, pos);
+    const int fadeStart = v.loopEnd - v.loopCrossfade;
+    if (v.loopEnd > 0 && v.loopCrossfade > 0 && pos >= fadeStart) {
+        const float2 entry = sincAt(bank, sinc, v, pos - period);
+        const float phase = float((pos - fadeStart) / v.loopCrossfade);
+        const float blend = .5f - .5f * cosf(3.14159265358979323846f * phase);
+        sample.x = fmaf(blend, entry.x - sample.x, sample.x);
+        sample.y = fmaf(blend, entry.y - sample.y, sample.y);
+    }
+    return sample;
+}
+
+__device__ __forceinline__ short toPcm16(float value)
+{
+    return short(__float2int_rn(fminf(32767.f, fmaxf(-32768.f, value * 32768.f))));
+}
+
+// Constant-power pan gains (render.cu:130-136).
+__device__ __forceinline__ float2 panGains(const cs_voice_span& v, float offset)
+{
+    if (offset == 0)
+        return make_float2(v.left, v.right);
+    const float p = fminf(1.f, fmaxf(-1.f, v.pan + offset));
+    return make_float2(v.gain * cosf((1 + p) * kQuarterPi), v.gain * cosf((1 - p) * kQuarterPi));
+}
+
+// Enveloped, modulated, panned voice frame (render.cu:138-187).  With
+// `filterInput`, mono sources are returned before panning (the mix pans them
+// after the filter).
+__device__ __forceinline__ float2 voiceFrame(const float* __restrict__ bank, const float* __restrict__ sinc,
+                                             const cs_voice_span& v, const cs_control_point* __restrict__ points,
+                                             const cs_voice_modulation* __restrict__ modulation, float pan,
+                                             int frame, bool filterInput, double phase)
+{
+    float level = envelopeAt(v, frame);
+    if (level <= 0)
+        return make_float2(0.f, 0.f);
+    float db = 0, widthOffset = 0, positionOffset = 0;
+    const int modEnd = v.firstModulation + v.modulationCount;
+    for (int j = v.firstModulation; j < modEnd; ++j) {
+        const cs_voice_modulation m = modulation[j];
+        if (m.target > CS_MOD_POSITION)
+            continue;
+        const float value = bindingAt(m, points, frame);
+        switch (m.target) {
+        case CS_MOD_AMPLITUDE: level *= value; break;
+        case CS_MOD_VOLUME: db += value; break;
+        case CS_MOD_PAN: pan += value; break;
+        case CS_MOD_WIDTH: widthOffset += value; break;
+        case CS_MOD_POSITION: positionOffset += value; break;
+        default: break;
+        }
+    }
+    if (db != 0)
+        level *= exp2f(db * .166096404744368f);
+    const float2 sample = voiceSource(bank, sinc, v, frame, phase);
+    if (filterInput && v.channels == 1)
+        return make_float2(sample.x * level, sample.x * level);
+    const float2 gains = panGains(v, pan);
+    const float l = sample.x * gains.x;
+    const float r = sample.y * gains.y;
+    if (v.stereoMatrix) {
+        float direct = v.widthDirect, cross = v.widthCross;
+        if (widthOffset != 0) {
+            const float width = fminf(1.f, fmaxf(-1.f, v.width + widthOffset));
+            direct = cosf((1 - width) * kQuarterPi);
+            cross = cosf((1 + width) * kQuarterPi);
+        }
+        float positionLeft = v.positionLeft, positionRight = v.positionRight;
+        if (positionOffset != 0) {
+            const float position = fminf(1.f, fmaxf(-1.f, v.stereoPosition + positionOffset));
+            positionLeft = cosf((1 + position) * kQuarterPi);
+            positionRight = cosf((1 - position) * kQuarterPi);
+        }
+        return make_float2(fmaf(r, cross, l * direct) * (level * positionLeft),
+                           fmaf(l, cross, r * direct) * (level * positionRight));
+    }
+    return make_float2(l * level, r * level);
+}
+
+// ---- filters (render.cu:276-336) ------------------------------------------------
+
+struct Biquad {
+    float b0, b1, b2, a1, a2;
+};
+
+__device__ __forceinline__ Biquad designFilter(int type, float cutoff, float resonance, int rate, float bandwidth,
+                                               float gain)
+{
+    const float w = 6.28318530717958647692f * fminf(fminf(20000.f, float(rate) * .499f), fmaxf(1.f, cutoff)) /
+        float(rate);
+    if (type == CS_FILTER_LOW1 || type == CS_FILTER_HIGH1) {
+        const float p = expf(-w);
+        if (type == CS_FILTER_LOW1)
+            return {1 - p, 0, 0, -p, 0};
+        const float high = (1 + p) * .5f;
+        return {high, -high, 0, -p, 0};
+    }
+    float s, c;
+    sincosf(w, &s, &c);
+    if (type == CS_FILTER_PEAK) {
+        const float a = exp2f(fminf(60.f, fmaxf(-96.f, gain)) * .083048202372184f);
+        const float width = fminf(12.f, fmaxf(.01f, bandwidth));
+        const float alpha = s * sinhf(fminf(20.f, .346573590279973f * width * w / s));
+        const float inv = 1 / (1 + alpha / a);
+        const float mid = -2 * c * inv;
+        return {(1 + alpha * a) * inv, mid, (1 - alpha * a) * inv, mid, (1 - alpha / a) * inv};
+    }
+    const float alpha = .5f * s * exp2f(-.166096404744368f * fminf(60.f, fmaxf(-60.f, resonance)));
+    const float inv = 1.f / (1 + alpha);
+    const float a1 = -2 * c * inv;
+    const float a2 = (1 - alpha) * inv;
+    if (type == CS_FILTER_BAND2 || type == CS_FILTER_BAND4 || type == CS_FILTER_BAND6)
+        return {alpha * inv, 0, -alpha * inv, a1, a2};
+    if (type == CS_FILTER_NOTCH2)
+        return {inv, a1, inv, a1, a2};
+    const bool high = type == CS_FILTER_HIGH2 || type == CS_FILTER_HIGH4 || type == CS_FILTER_HIGH6;
+    const float b = (1 + (high ? c : -c)) * .5f * inv;
+    return {b, (high ? -2 : 2) * b, b, a1, a2};
+}
+
+__device__ __forceinline__ int filterSections(int type)
+{
+    if (type == CS_FILTER_NONE) return 0;
+    if (type == CS_FILTER_PEAK) return 1;
+    if (type >= CS_FILTER_LOW6) return 3;
+    if (type >= CS_FILTER_LOW4) return 2;
+    return 1;
+}
+
+__device__ __forceinline__ void smoothToward(Biquad& current, const Biquad& target, float amount)
+{
+    current.b0 = fmaf(amount, target.b0 - current.b0, current.b0);
+    current.b1 = fmaf(amount, target.b1 - current.b1, current.b1);
+    current.b2 = fmaf(amount, target.b2 - current.b2, current.b2);
+    current.a1 = fmaf(amount, target.a1 - current.a1, current.a1);
+    current.a2 = fmaf(amount, target.a2 - current.a2, current.a2);
+}
+
+// Transposed direct form II step.
+__device__ __forceinline__ float biquadStep(float x, const Biquad& c, float& z1, float& z2)
+{
+    const float y = fmaf(c.b0, x, z1);
+    z1 = fmaf(-c.a1, y, fmaf(c.b1, x, z2));
+    z2 = fmaf(-c.a2, y, c.b2 * x);
+    return y;
+}
+
+// True when a span's filter coefficients change per frame (render.cu:370-375).
+__device__ __forceinline__ bool filterMoves(const cs_voice_span& v, const cs_voice_modulation* __restrict__ modulation)
+{
+    bool moving = v.activeEnvelope[0] != 0;
+    for (int j = v.firstModulation; j < v.firstModulation + v.modulationCount; ++j) {
+        const int target = modulation[j].target;
+        moving |= (target >= CS_MOD_CUTOFF && target <= CS_MOD_RESONANCE2) || target == CS_MOD_FILEG_DEPTH ||
+            target >= CS_MOD_EQ1_FREQUENCY;
+    }
+    return moving;
+}
+
+// Target coefficients of every filter slot at `frame` (render.cu:378-405).
+__device__ __forceinline__ void filterTargets(const cs_voice_span& v, const cs_control_point* __restrict__ points,
+                                              const cs_voice_modulation* __restrict__ modulation, int frame,
+                                              Biquad* out)
+{
+    float cents[2] = {0, 0}, db[2] = {0, 0};
+    float eq[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    float depth = v.extraEnvelope[0].depth;
+    for (int j = v.firstModulation; j < v.firstModulation + v.modulationCount; ++j) {
+        const cs_voice_modulation m = modulation[j];
+        if (m.target == CS_MOD_CUTOFF) cents[0] += bindingAt(m, points, frame);
+        if (m.target == CS_MOD_CUTOFF2) cents[1] += bindingAt(m, points, frame);
+        if (m.target == CS_MOD_RESONANCE) db[0] += bindingAt(m, points, frame);
+        if (m.target == CS_MOD_RESONANCE2) db[1] += bindingAt(m, points, frame);
+        if (m.target == CS_MOD_FILEG_DEPTH) depth += bindingAt(m, points, frame);
+        if (m.target >= CS_MOD_EQ1_FREQUENCY) {
+            const int id = m.target - CS_MOD_EQ1_FREQUENCY;
+            eq[id / 3][id % 3] += bindingAt(m, points, frame);
+        }
+    }
+    if (v.activeEnvelope[0])
+        cents[0] += depth * envelopeAt(v.extraEnvelope[0], frame);
+    for (int f = 0; f < CS_FILTER_SLOTS; ++f) {
+        const cs_voice_filter& filter = v.filters[f];
+        if (!filterSections(filter.type))
+            continue;
+        out[f] = f < 2 ? designFilter(filter.type, filter.cutoff * exp2f(cents[f] / 1200), filter.resonance + db[f],
+                                      v.sampleRate, 0, 0)
+                       : designFilter(filter.type, filter.cutoff + eq[f - 2][0], 0, v.sampleRate,
+                                      filter.bandwidth + eq[f - 2][1], filter.gain + eq[f - 2][2]);
+    }
+}
+
+} // namespace cs

@@ -1,0 +1,161 @@
+"""Planned render jobs as numpy arrays.
+
+A :class:`Plan` holds one job's ``cs_plan`` arrays (the reference's
+``clay::RenderPlan``, src/render/plan.h:9-20).  The record dtypes below are
+byte-compatible with the C structs in ``include/claysampler_b200.h`` (and with the
+reference's src/cuda/render_types.h), so arrays pass through ctypes unchanged.
+"""
+from __future__ import annotations
+
+import ctypes
+import struct
+from dataclasses import dataclass, field
+
+import numpy as np
+
+VOICE_FILTER = np.dtype([("type", "<i4"), ("cutoff", "<f4"), ("resonance", "<f4"),
+                         ("bandwidth", "<f4"), ("gain", "<f4")], align=True)
+ENVELOPE_SHAPE = np.dtype(
+    [(n, "<i4") for n in ("attackStart", "holdStart", "decayStart", "releaseStart", "fadeStart")]
+    + [(n, "<f4") for n in ("start", "attackStep", "decayRate", "sustain", "releaseValue", "releaseRate",
+                             "fadeValue", "fadeStep", "depth", "releaseSeconds")], align=True)
+VOICE_SPAN = np.dtype(
+    [("sample", "<u8"), ("position", "<f8"), ("step", "<f8"), ("pitchSlope", "<f8")]
+    + [(n, "<i4") for n in ("channels", "begin", "end", "sourceEnd", "loopFirst", "loopEnd", "loopCrossfade",
+                             "stereoMatrix", "generator")]
+    + [("noiseSeed", "<u4")]
+    + [(n, "<i4") for n in ("noiseStart", "firstModulation", "modulationCount", "firstLfo", "lfoCount",
+                             "filterTrack", "nextFilteredSpan")]
+    + [("filteredOffset", "<u8"), ("phaseOffset", "<u8"), ("variablePitch", "<i4"), ("minimumPitchRatio", "<f4"),
+       ("filterControls", "<i4", (4,)), ("sampleRate", "<i4"), ("filters", VOICE_FILTER, (5,)),
+       ("extraEnvelope", ENVELOPE_SHAPE, (2,)), ("activeEnvelope", "<i4", (2,))]
+    + [(n, "<i4") for n in ("attackStart", "holdStart", "decayStart", "releaseStart", "fadeStart", "bendEnd")]
+    + [(n, "<f4") for n in ("gain", "pan", "left", "right", "start", "attackStep", "decayRate", "sustain",
+                             "releaseValue", "releaseRate", "fadeValue", "fadeStep", "widthDirect", "widthCross",
+                             "positionLeft", "positionRight", "width", "stereoPosition")], align=True)
+CONTROL_POINT = np.dtype([("frame", "<i4"), ("value", "<f4"), ("step", "<f4")], align=True)
+VOICE_MODULATION = np.dtype([("first", "<i4"), ("last", "<i4"), ("target", "<i4"), ("depth", "<f4"),
+                             ("shapeFirst", "<i4"), ("shapeLast", "<i4")], align=True)
+AUDIO_METRICS = np.dtype([(n, "<f8") for n in ("median", "quartile", "silentFraction", "clippedFraction",
+                                                "bodyRms", "targetRms", "gain")]
+                         + [("longestSilence", "<i4"), ("clipped", "<i4"), ("verdict", "<i4"),
+                            ("measured", "u1")], align=True)
+TAIL_RESULT = np.dtype([("offset", "<u8")]
+                       + [(n, "<i4") for n in ("frames", "dataFrames", "fade", "peak", "first", "last", "status")]
+                       + [("scale", "<f4"), ("audio", AUDIO_METRICS)], align=True)
+AUDIO_CONFIG = np.dtype([(n, "<i4") for n in ("rate", "window", "maxFrames", "minPeak")] + [("enabled", "u1")]
+                        + [(n, "<f8") for n in ("minMedian", "minQuartile", "silencePower", "maxSilentFraction",
+                                                 "maxSilentFrames", "maxClippedFraction")], align=True)
+
+assert VOICE_SPAN.itemsize == 472 and CONTROL_POINT.itemsize == 12
+assert VOICE_MODULATION.itemsize == 24 and TAIL_RESULT.itemsize == 112 and AUDIO_CONFIG.itemsize == 72
+
+TAIL_STATUS = ["ok", "duration", "nonfinite", "peak", "audioDuration", "quietPerformance", "excessiveSilence",
+               "silentAudio", "clipping", "silentBody", "incompleteGroup", "scratchMemory"]
+
+_HEADER = struct.Struct("<4sI12iQQ")
+
+
+class CPlan(ctypes.Structure):
+    """ctypes mirror of ``cs_plan``."""
+    _fields_ = [("spans", ctypes.c_void_p), ("points", ctypes.c_void_p), ("track_offsets", ctypes.c_void_p),
+                ("modulation", ctypes.c_void_p), ("onsets", ctypes.c_void_p),
+                ("span_count", ctypes.c_int32), ("track_count", ctypes.c_int32),
+                ("modulation_count", ctypes.c_int32), ("onset_count", ctypes.c_int32),
+                ("filter_tracks", ctypes.c_int32), ("frames", ctypes.c_int32), ("music_end", ctypes.c_int32),
+                ("limit", ctypes.c_int32), ("fade_frames", ctypes.c_int32), ("tail_clipped", ctypes.c_int32),
+                ("body_frames", ctypes.c_int32), ("volume_group", ctypes.c_uint64)]
+
+
+@dataclass
+class Plan:
+    spans: np.ndarray
+    points: np.ndarray
+    track_offsets: np.ndarray
+    modulation: np.ndarray
+    onsets: np.ndarray
+    filter_tracks: int = 0
+    frames: int = 0
+    music_end: int = 0
+    limit: int = 0
+    fade_frames: int = 0
+    tail_clipped: int = 0
+    body_frames: int = 0
+    volume_group: int = 0
+    _keep: list = field(default_factory=list, repr=False)
+
+    @classmethod
+    def from_blob(cls, blob: bytes) -> "Plan":
+        (magic, version, filter_tracks, frames, music_end, limit, fade_frames, tail_clipped, body_frames,
+         spans, tracks, mods, onsets, _, group, points) = _HEADER.unpack_from(blob, 0)
+        if magic != b"CSPL" or version != 1:
+            raise ValueError("not a plan image")
+        offset = _HEADER.size
+
+        def take(dtype, count):
+            nonlocal offset
+            array = np.frombuffer(blob, dtype=dtype, count=count, offset=offset).copy()
+            offset += array.nbytes
+            return array
+        plan = cls(take(VOICE_SPAN, spans), None, None, None, None, filter_tracks, frames, music_end, limit,
+                   fade_frames, tail_clipped, body_frames, group)
+        plan.track_offsets = take(np.int64, tracks + 1)
+        plan.points = take(CONTROL_POINT, points)
+        plan.modulation = take(VOICE_MODULATION, mods)
+        plan.onsets = take(np.int32, onsets)
+        if offset != len(blob):
+            raise ValueError("truncated plan image")
+        return plan
+
+    def to_blob(self) -> bytes:
+        head = _HEADER.pack(b"CSPL", 1, self.filter_tracks, self.frames, self.music_end, self.limit,
+                            self.fade_frames, self.tail_clipped, self.body_frames, len(self.spans),
+                            len(self.track_offsets) - 1, len(self.modulation), len(self.onsets), 0,
+                            self.volume_group, len(self.points))
+        return b"".join([head, self.spans.tobytes(), self.track_offsets.astype(np.int64).tobytes(),
+                         self.points.tobytes(), self.modulation.tobytes(), self.onsets.astype(np.int32).tobytes()])
+
+    @property
+    def track_count(self) -> int:
+        return len(self.track_offsets) - 1
+
+    def track(self, index: int) -> np.ndarray:
+        return self.points[self.track_offsets[index]:self.track_offsets[index + 1]]
+
+    def as_c(self) -> CPlan:
+        arrays = [np.ascontiguousarray(a) for a in (self.spans, self.points, self.track_offsets.astype(np.int64),
+                                                    self.modulation, self.onsets.astype(np.int32))]
+        self._keep = arrays
+        ptr = [a.ctypes.data if a.size else None for a in arrays]
+        return CPlan(ptr[0], ptr[1], ptr[2], ptr[3], ptr[4], len(self.spans), self.track_count,
+                     len(self.modulation), len(self.onsets), self.filter_tracks, self.frames, self.music_end,
+                     self.limit, self.fade_frames, self.tail_clipped, self.body_frames, self.volume_group)
+
+    def voice_frames(self) -> int:
+        return int(np.sum(self.spans["end"].astype(np.int64) - self.spans["begin"]))
+
+
+def c_plans(plans: list[Plan]):
+    """A ctypes array of ``cs_plan`` views (the plans keep their buffers alive)."""
+    array = (CPlan * len(plans))()
+    for i, plan in enumerate(plans):
+        array[i] = plan.as_c()
+    return array
+
+
+def default_audio_config(rate: int = 44100, quality: bool = False) -> np.ndarray:
+    """audioConfig() of the reference CLI (src/main.cpp:169-187)."""
+    power = lambda dbfs: 4294967296.0 * 10.0 ** (dbfs / 10)  # noqa: E731
+    config = np.zeros((), AUDIO_CONFIG)
+    config["rate"] = rate
+    config["window"] = int(np.rint(rate / 20.0))
+    config["maxFrames"] = 375 * rate
+    config["minPeak"] = 32
+    config["enabled"] = 1 if quality else 0
+    config["minMedian"] = -38
+    config["minQuartile"] = -45
+    config["silencePower"] = power(-70)
+    config["maxSilentFraction"] = 0.75
+    config["maxSilentFrames"] = 10.0 * rate
+    config["maxClippedFraction"] = 0.0001
+    return config

@@ -1,0 +1,236 @@
+"""Python mirror of the reference's ``clay::Renderer`` (src/cuda/renderer.h:45-64).
+
+The class wraps the C ABI of ``libclaysampler_b200.so`` (``include/claysampler_b200.h``)
+with the same operations: ``upload_samples``, ``render_window`` with a publish
+callback and an optional refill callback, and the memory getters.  There is no
+fallback: if the CUDA library is missing or no sm_100 GPU is present, construction
+raises.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from pathlib import Path
+from typing import Callable, Optional
+
+import numpy as np
+
+from . import build
+from .plans import AUDIO_CONFIG, TAIL_RESULT, CPlan, Plan, c_plans, default_audio_config
+
+_lib = None
+
+
+def library() -> ctypes.CDLL:
+    """Load (building first if stale) the in-tree CUDA library."""
+    global _lib
+    if _lib is None:
+        path = build.LIBRARY
+        if not path.exists():
+            build.build_library()
+        lib = ctypes.CDLL(str(path))
+        c = ctypes
+        vp, sz, i32 = c.c_void_p, c.c_size_t, c.c_int
+        lib.cs_last_error.restype = c.c_char_p
+        lib.cs_renderer_create.argtypes = [i32, i32, vp, i32, sz, sz, c.POINTER(vp)]
+        lib.cs_renderer_destroy.argtypes = [vp]
+        lib.cs_upload_samples.argtypes = [vp, vp, sz, i32]
+        lib.cs_render_window.argtypes = [vp, vp, sz, vp, vp, vp]
+        lib.cs_renderer_device.argtypes = [vp]
+        lib.cs_renderer_device.restype = c.c_char_p
+        for name in ("cs_peak_bytes", "cs_sample_cache_budget", "cs_peak_waiting_bytes", "cs_spilled_bytes",
+                     "cs_downloaded_bytes"):
+            getattr(lib, name).argtypes = [vp]
+            getattr(lib, name).restype = sz
+        lib.cs_prepare.argtypes = [vp, vp, sz, c.POINTER(vp)]
+        lib.cs_run.argtypes = [vp, vp, vp]
+        lib.cs_collect.argtypes = [vp, vp, vp, sz, c.POINTER(sz), vp]
+        lib.cs_copy_mix.argtypes = [vp, vp, vp, sz]
+        lib.cs_prepared_frames.argtypes = [vp]
+        lib.cs_prepared_frames.restype = sz
+        lib.cs_prepared_launches.argtypes = [vp]
+        lib.cs_prepared_segments.argtypes = [vp]
+        lib.cs_prepared_segments.restype = sz
+        lib.cs_prepared_destroy.argtypes = [vp]
+        lib.cs_renderer_set_scratch_limit.argtypes = [vp, sz]
+        _lib = lib
+    return _lib
+
+
+def _check(status: int) -> None:
+    if status:
+        raise RuntimeError(library().cs_last_error().decode(errors="replace"))
+
+
+class CBatch(ctypes.Structure):
+    _fields_ = [("pcm", ctypes.c_void_p), ("pcm_samples", ctypes.c_size_t), ("results", ctypes.c_void_p),
+                ("result_count", ctypes.c_size_t), ("kernel_seconds", ctypes.c_double),
+                ("failed_scratch_bytes", ctypes.c_size_t), ("job_indices", ctypes.c_void_p),
+                ("job_index_count", ctypes.c_size_t)]
+
+
+PUBLISH = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.POINTER(CBatch), ctypes.c_size_t)
+REFILL = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                          ctypes.POINTER(ctypes.c_size_t))
+
+
+@dataclass
+class RenderBatch:
+    """clay::RenderBatch (src/cuda/renderer.h:37-43) with owned copies."""
+    pcm: np.ndarray
+    results: np.ndarray
+    kernel_seconds: float
+    failed_scratch_bytes: int
+    job_indices: list
+
+
+class Prepared:
+    """A staged batch whose inputs stay resident on the device."""
+
+    def __init__(self, renderer: "Renderer", plans: list[Plan]):
+        self.renderer = renderer
+        self.plans = plans
+        self._array = c_plans(plans)
+        handle = ctypes.c_void_p()
+        _check(library().cs_prepare(renderer.handle, self._array, len(plans), ctypes.byref(handle)))
+        self.handle = handle
+
+    @property
+    def frames(self) -> int:
+        return library().cs_prepared_frames(self.handle)
+
+    @property
+    def launches(self) -> int:
+        return library().cs_prepared_launches(self.handle)
+
+    @property
+    def segments(self) -> int:
+        return library().cs_prepared_segments(self.handle)
+
+    def run(self, stream: int | None = None) -> None:
+        _check(library().cs_run(self.renderer.handle, self.handle, stream))
+
+    def collect(self) -> tuple[np.ndarray, np.ndarray]:
+        samples = ctypes.c_size_t()
+        results = np.zeros(len(self.plans), TAIL_RESULT)
+        _check(library().cs_collect(self.renderer.handle, self.handle, None, 0, ctypes.byref(samples),
+                                    results.ctypes.data))
+        pcm = np.zeros(samples.value, np.int16)
+        _check(library().cs_collect(self.renderer.handle, self.handle, pcm.ctypes.data if pcm.size else None,
+                                    pcm.size, ctypes.byref(samples), results.ctypes.data))
+        return pcm, results
+
+    def mix(self) -> np.ndarray:
+        dtype = np.float32 if self.renderer.natural else np.int16
+        out = np.zeros((self.frames, 2), dtype)
+        _check(library().cs_copy_mix(self.renderer.handle, self.handle, out.ctypes.data, out.nbytes))
+        return out
+
+    def close(self) -> None:
+        if self.handle:
+            library().cs_prepared_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+
+class Renderer:
+    """clay::Renderer over the B200 kernels."""
+
+    def __init__(self, device: int = 0, natural: bool = True, audio: Optional[np.ndarray] = None,
+                 group_minimum: int = 0, waiting_limit: int = 256 << 20, batch_jobs: int = 64):
+        self.natural = natural
+        self.audio = default_audio_config() if audio is None else np.asarray(audio, AUDIO_CONFIG)
+        handle = ctypes.c_void_p()
+        _check(library().cs_renderer_create(device, int(natural), self.audio.ctypes.data, group_minimum,
+                                            waiting_limit, batch_jobs, ctypes.byref(handle)))
+        self.handle = handle
+        self._bank = None
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            library().cs_renderer_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+    def upload_samples(self, bank: np.ndarray, fresh: bool = False) -> None:
+        bank = np.ascontiguousarray(bank, np.float32)
+        self._bank = bank
+        _check(library().cs_upload_samples(self.handle, bank.ctypes.data if bank.size else None, bank.size,
+                                           int(fresh)))
+
+    def set_scratch_limit(self, nbytes: int) -> None:
+        _check(library().cs_renderer_set_scratch_limit(self.handle, nbytes))
+
+    def prepare(self, plans: list[Plan]) -> Prepared:
+        return Prepared(self, plans)
+
+    def render_window(self, plans: list[Plan], publish: Callable[[RenderBatch, int], None],
+                      refill: Optional[Callable[[bool], list[Plan]]] = None) -> None:
+        """Render every plan; ``publish(batch, first)`` receives each finished batch.
+
+        ``refill(wait)`` may return more plans (or an empty list when none are ready),
+        like the reference's Refill callback.
+        """
+        array = c_plans(plans)
+        keep = [array]
+        errors = []
+
+        def on_publish(_user, batch_ptr, first):
+            try:
+                b = batch_ptr.contents
+                pcm = np.ctypeslib.as_array(ctypes.cast(b.pcm, ctypes.POINTER(ctypes.c_int16)),
+                                            shape=(b.pcm_samples,)).copy() if b.pcm_samples else np.zeros(0, np.int16)
+                results = np.frombuffer(ctypes.string_at(b.results, b.result_count * TAIL_RESULT.itemsize),
+                                        TAIL_RESULT).copy() if b.result_count else np.zeros(0, TAIL_RESULT)
+                indices = [ctypes.cast(b.job_indices, ctypes.POINTER(ctypes.c_size_t))[i]
+                           for i in range(b.job_index_count)] if b.job_index_count else []
+                publish(RenderBatch(pcm, results, b.kernel_seconds, b.failed_scratch_bytes, indices), first)
+            except Exception as exc:  # surfaced after the C call returns
+                errors.append(exc)
+
+        def on_refill(_user, wait, plans_out, count_out):
+            if refill is None:
+                return 0
+            more = refill(bool(wait))
+            if not more:
+                return 0
+            extra = c_plans(more)
+            keep.append((extra, more))
+            plans_out[0] = ctypes.cast(extra, ctypes.c_void_p)
+            count_out[0] = len(more)
+            return 1
+
+        publish_cb, refill_cb = PUBLISH(on_publish), REFILL(on_refill)
+        status = library().cs_render_window(self.handle, array, len(plans), ctypes.cast(publish_cb, ctypes.c_void_p),
+                                            ctypes.cast(refill_cb, ctypes.c_void_p), None)
+        if errors:
+            raise errors[0]
+        _check(status)
+
+    @property
+    def device(self) -> str:
+        return library().cs_renderer_device(self.handle).decode()
+
+    @property
+    def peak_bytes(self) -> int:
+        return library().cs_peak_bytes(self.handle)
+
+    @property
+    def sample_cache_budget(self) -> int:
+        return library().cs_sample_cache_budget(self.handle)
+
+    @property
+    def peak_waiting_bytes(self) -> int:
+        return library().cs_peak_waiting_bytes(self.handle)
+
+    @property
+    def spilled_bytes(self) -> int:
+        return library().cs_spilled_bytes(self.handle)
+
+    @property
+    def downloaded_bytes(self) -> int:
+        return library().cs_downloaded_bytes(self.handle)

@@ -1,0 +1,239 @@
+/*
+ * claysampler_b200 — C ABI of the B200 batch voice renderer.
+ *
+ * The renderer is a drop-in for ClaySampler's device half: the planner hands it
+ * one `cs_plan` per job (the reference's `clay::RenderPlan`, src/render/plan.h:9-20)
+ * and it returns PCM16 plus one `cs_tail_result` per job (the reference's
+ * `clay::RenderBatch`, src/cuda/renderer.h:37-43).  All entry points return 0 on
+ * success and a nonzero status on failure; `cs_last_error` gives the message
+ * (the reference throws std::runtime_error from Driver::check,
+ * src/cuda/renderer.cpp:69-77, which its CLI turns into `ERROR\t...`, exit 1).
+ *
+ * The POD records below are byte-compatible with the reference's shared host/device
+ * structs in src/cuda/render_types.h, so a planner built against either header can
+ * pass its arrays through unchanged.  Field names follow the reference.
+ */
+#ifndef CLAYSAMPLER_B200_H
+#define CLAYSAMPLER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- enumerations (src/cuda/render_types.h:3-15, 105-108) ---------------------- */
+enum cs_mod_target {
+    CS_MOD_AMPLITUDE, CS_MOD_VOLUME, CS_MOD_PAN, CS_MOD_WIDTH, CS_MOD_POSITION, CS_MOD_PITCH,
+    CS_MOD_ENV_DELAY, CS_MOD_ENV_ATTACK, CS_MOD_ENV_HOLD, CS_MOD_ENV_DECAY, CS_MOD_ENV_SUSTAIN,
+    CS_MOD_ENV_START, CS_MOD_ENV_RELEASE, CS_MOD_OFFSET, CS_MOD_DELAY,
+    CS_MOD_CUTOFF, CS_MOD_RESONANCE, CS_MOD_CUTOFF2, CS_MOD_RESONANCE2,
+    CS_MOD_FILTER_VELOCITY, CS_MOD_FILTER_VELOCITY2,
+    CS_MOD_LFO_FREQUENCY, CS_MOD_LFO_PHASE, CS_MOD_LFO_DELAY, CS_MOD_LFO_FADE,
+    CS_MOD_FILEG_DELAY, CS_MOD_FILEG_ATTACK, CS_MOD_FILEG_HOLD, CS_MOD_FILEG_DECAY,
+    CS_MOD_FILEG_SUSTAIN, CS_MOD_FILEG_START, CS_MOD_FILEG_RELEASE,
+    CS_MOD_PITCHEG_DELAY, CS_MOD_PITCHEG_ATTACK, CS_MOD_PITCHEG_HOLD, CS_MOD_PITCHEG_DECAY,
+    CS_MOD_PITCHEG_SUSTAIN, CS_MOD_PITCHEG_START, CS_MOD_PITCHEG_RELEASE,
+    CS_MOD_FILEG_DEPTH, CS_MOD_PITCHEG_DEPTH,
+    CS_MOD_EQ1_FREQUENCY, CS_MOD_EQ1_BANDWIDTH, CS_MOD_EQ1_GAIN,
+    CS_MOD_EQ2_FREQUENCY, CS_MOD_EQ2_BANDWIDTH, CS_MOD_EQ2_GAIN,
+    CS_MOD_EQ3_FREQUENCY, CS_MOD_EQ3_BANDWIDTH, CS_MOD_EQ3_GAIN
+};
+
+enum cs_filter_type {
+    CS_FILTER_NONE, CS_FILTER_LOW1, CS_FILTER_HIGH1, CS_FILTER_LOW2, CS_FILTER_HIGH2,
+    CS_FILTER_BAND2, CS_FILTER_NOTCH2, CS_FILTER_LOW4, CS_FILTER_HIGH4, CS_FILTER_BAND4,
+    CS_FILTER_LOW6, CS_FILTER_HIGH6, CS_FILTER_BAND6, CS_FILTER_PEAK
+};
+
+enum cs_generator { CS_GEN_NONE, CS_GEN_SINE, CS_GEN_SILENCE, CS_GEN_NOISE };
+
+enum cs_tail_status {
+    CS_TAIL_OK, CS_TAIL_DURATION, CS_TAIL_NONFINITE, CS_TAIL_PEAK, CS_TAIL_AUDIO_DURATION,
+    CS_TAIL_QUIET_PERFORMANCE, CS_TAIL_EXCESSIVE_SILENCE, CS_TAIL_SILENT_AUDIO, CS_TAIL_CLIPPING,
+    CS_TAIL_SILENT_BODY, CS_TAIL_INCOMPLETE_GROUP, CS_TAIL_SCRATCH_MEMORY
+};
+
+#define CS_FILTER_SLOTS 5
+#define CS_TAIL_BLOCK_FRAMES 1024      /* src/cuda/render_types.h:92 */
+#define CS_NATURAL_TAIL_LIMIT_SECONDS 120
+
+/* ---- plan records (src/cuda/render_types.h:30-90) -------------------------------- */
+typedef struct cs_voice_filter {
+    int32_t type;                        /* enum cs_filter_type */
+    float cutoff, resonance, bandwidth, gain;
+} cs_voice_filter;
+
+typedef struct cs_envelope_shape {
+    int32_t attackStart, holdStart, decayStart, releaseStart, fadeStart;
+    float start, attackStep, decayRate, sustain, releaseValue, releaseRate, fadeValue, fadeStep;
+    float depth, releaseSeconds;
+} cs_envelope_shape;
+
+/* One contiguous span of one voice (src/cuda/render_types.h:41-68), 472 bytes. */
+typedef struct cs_voice_span {
+    uint64_t sample;                     /* offset of frame 0 in the float bank */
+    double position, step, pitchSlope;
+    int32_t channels, begin, end, sourceEnd, loopFirst, loopEnd, loopCrossfade;
+    int32_t stereoMatrix;
+    int32_t generator;                   /* enum cs_generator */
+    uint32_t noiseSeed;
+    int32_t noiseStart;
+    int32_t firstModulation, modulationCount;
+    int32_t firstLfo, lfoCount;
+    int32_t filterTrack, nextFilteredSpan;
+    uint64_t filteredOffset, phaseOffset;
+    int32_t variablePitch;
+    float minimumPitchRatio;
+    int32_t filterControls[4];
+    int32_t sampleRate;
+    cs_voice_filter filters[CS_FILTER_SLOTS];
+    cs_envelope_shape extraEnvelope[2];
+    int32_t activeEnvelope[2];
+    int32_t attackStart, holdStart, decayStart, releaseStart, fadeStart, bendEnd;
+    float gain, pan, left, right, start, attackStep, decayRate, sustain, releaseValue, releaseRate;
+    float fadeValue, fadeStep;
+    float widthDirect, widthCross, positionLeft, positionRight;
+    float width, stereoPosition;
+} cs_voice_span;
+
+/* Piecewise-linear control track point (src/cuda/render_types.h:76-79). */
+typedef struct cs_control_point {
+    int32_t frame;
+    float value, step;
+} cs_control_point;
+
+/* Modulation binding (src/cuda/render_types.h:81-86).  In a plan, `first` and
+ * `shapeFirst` are track indices (or -1); the renderer rebases them to points. */
+typedef struct cs_voice_modulation {
+    int32_t first, last;
+    int32_t target;                      /* enum cs_mod_target */
+    float depth;
+    int32_t shapeFirst, shapeLast;
+} cs_voice_modulation;
+
+/* Quality-gate configuration (src/cuda/render_types.h:110-114). */
+typedef struct cs_audio_config {
+    int32_t rate, window, maxFrames, minPeak;
+    uint8_t enabled;
+    double minMedian, minQuartile, silencePower, maxSilentFraction, maxSilentFrames, maxClippedFraction;
+} cs_audio_config;
+
+typedef struct cs_audio_metrics {
+    double median, quartile, silentFraction, clippedFraction, bodyRms, targetRms, gain;
+    int32_t longestSilence, clipped;
+    int32_t verdict;                     /* enum cs_tail_status */
+    uint8_t measured;
+} cs_audio_metrics;
+
+/* Per-job result (src/cuda/render_types.h:134-140), 112 bytes. */
+typedef struct cs_tail_result {
+    uint64_t offset;                     /* first frame of this job in the batch PCM */
+    int32_t frames, dataFrames, fade, peak, first, last;
+    int32_t status;                      /* enum cs_tail_status */
+    float scale;
+    cs_audio_metrics audio;
+} cs_tail_result;
+
+/* One render job (clay::RenderPlan, src/render/plan.h:9-20) as flat arrays.
+ * Control track i is points[track_offsets[i] .. track_offsets[i+1]).  Tracks 0..2
+ * are the job's CC7, CC11 and CC10 automation (src/render/plan.cpp:296-305). */
+typedef struct cs_plan {
+    const cs_voice_span* spans;
+    const cs_control_point* points;
+    const int64_t* track_offsets;        /* track_count + 1 entries */
+    const cs_voice_modulation* modulation;
+    const int32_t* onsets;
+    int32_t span_count, track_count, modulation_count, onset_count;
+    int32_t filter_tracks, frames, music_end, limit, fade_frames, tail_clipped, body_frames;
+    uint64_t volume_group;
+} cs_plan;
+
+/* ---- renderer (clay::Renderer, src/cuda/renderer.h:45-64) ---------------------- */
+typedef struct cs_renderer cs_renderer;
+
+/* A finished batch (clay::RenderBatch).  `pcm` holds result.dataFrames frames per
+ * accepted job starting at result.offset, mono in natural mode and interleaved
+ * stereo otherwise; it stays valid only during the publish callback. */
+typedef struct cs_batch {
+    const int16_t* pcm;
+    size_t pcm_samples;
+    const cs_tail_result* results;
+    size_t result_count;
+    double kernel_seconds;
+    size_t failed_scratch_bytes;         /* single rejected job at `first` */
+    const size_t* job_indices;           /* noncontiguous completions, else NULL */
+    size_t job_index_count;
+} cs_batch;
+
+typedef void (*cs_publish_fn)(void* user, const cs_batch* batch, size_t first);
+/* Appends more plans while rendering (clay::Renderer::Refill).  Returns 1 and sets
+ * `plans`/`count` to an array that stays valid until the renderer publishes those
+ * jobs, or returns 0 when nothing is ready (`wait` = 0) or no work remains. */
+typedef int (*cs_refill_fn)(void* user, int wait, const cs_plan** plans, size_t* count);
+
+/* Replaces Renderer::Renderer (src/cuda/renderer.h:47-48, renderer.cpp:491-546).
+ * `natural` selects the float mix with natural-tail finishing (mono PCM16);
+ * otherwise the mix is stereo PCM16 (orig/custom).  No NVRTC path: the kernels are
+ * compiled offline for sm_100a. */
+int cs_renderer_create(int device, int natural, const cs_audio_config* audio, int group_minimum,
+                       size_t waiting_limit, size_t batch_jobs, cs_renderer** out);
+void cs_renderer_destroy(cs_renderer* renderer);
+
+/* Replaces Renderer::uploadSamples (src/cuda/renderer.cpp:553-603): the bank is
+ * interleaved float32; only the tail beyond the last upload is copied unless
+ * `fresh` restarts the bank. */
+int cs_upload_samples(cs_renderer* renderer, const float* pcm, size_t floats, int fresh);
+
+/* Replaces Renderer::renderWindow (src/cuda/renderer.cpp:1748-1820): renders every
+ * plan and calls `publish` once per finished batch with the index of its first job. */
+int cs_render_window(cs_renderer* renderer, const cs_plan* plans, size_t count,
+                     cs_publish_fn publish, cs_refill_fn refill, void* user);
+
+/* Getters (src/cuda/renderer.h:54-59). */
+const char* cs_renderer_device(const cs_renderer* renderer);
+size_t cs_peak_bytes(const cs_renderer* renderer);
+size_t cs_sample_cache_budget(const cs_renderer* renderer);
+size_t cs_peak_waiting_bytes(const cs_renderer* renderer);
+size_t cs_spilled_bytes(const cs_renderer* renderer);
+size_t cs_downloaded_bytes(const cs_renderer* renderer);
+
+/* Message of the last failed call on this thread (no reference counterpart: the
+ * reference reports failures as C++ exceptions). */
+const char* cs_last_error(void);
+
+/* ---- staged batches (measurement and tests; no reference counterpart) -----------
+ * A prepared batch keeps its plans' device metadata, mix and finishing buffers
+ * resident so that the synthesis + finishing pass can be re-run on device-resident
+ * inputs, the boundary at which kernel throughput is measured. */
+typedef struct cs_prepared cs_prepared;
+
+int cs_prepare(cs_renderer* renderer, const cs_plan* plans, size_t count, cs_prepared** out);
+/* Enqueues synthesis and finishing on `stream` (a cudaStream_t, NULL = the
+ * renderer's stream); does not synchronise. */
+int cs_run(cs_renderer* renderer, cs_prepared* batch, void* stream);
+/* Synchronises and copies results; `pcm` may be NULL to query `*pcm_samples`. */
+int cs_collect(cs_renderer* renderer, cs_prepared* batch, int16_t* pcm, size_t pcm_capacity,
+               size_t* pcm_samples, cs_tail_result* results);
+/* Copies the synthesised mix (float2 per frame in natural mode, short2 otherwise)
+ * for all jobs, concatenated in plan order. */
+int cs_copy_mix(cs_renderer* renderer, cs_prepared* batch, void* host, size_t bytes);
+size_t cs_prepared_frames(const cs_prepared* batch);
+/* Kernel launches the last cs_run enqueued. */
+int cs_prepared_launches(const cs_prepared* batch);
+void cs_prepared_destroy(cs_prepared* batch);
+/* Number of synthesis segments the batch was cut into. */
+size_t cs_prepared_segments(const cs_prepared* batch);
+
+/* Caps the chain-storage bytes of one synthesis segment (0 = derive the budget
+ * from free device memory).  No reference counterpart: the reference exercises
+ * segmentation with a special build that limits scratch to 64 KiB
+ * (docs/validation.md:145). */
+int cs_renderer_set_scratch_limit(cs_renderer* renderer, size_t bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

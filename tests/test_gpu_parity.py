@@ -1,0 +1,101 @@
+"""GPU parity: the sm_100a render path against the reference's own host render
+(oracle/_ref: the reference planner and src/cuda/render.cu compiled for the CPU)
+and the plain-C restatement of its finishing stages (oracle/).
+
+Tolerances (the contract for this path): float bus max |error| <= 1e-5 of full
+scale; PCM16 within 1 LSB with >= 99.9 % of samples identical; tail frame indices,
+output lengths and statuses bit-exact.
+"""
+import numpy as np
+import pytest
+
+from conftest import gpu_available
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not gpu_available(), reason="needs a CUDA GPU")]
+
+BUS_TOLERANCE = 1e-5
+PCM_IDENTICAL = 0.999
+
+
+def render(plans, bank, natural=True, scratch_limit=0):
+    from claysampler_b200.renderer import Renderer
+    renderer = Renderer(natural=natural)
+    renderer.upload_samples(bank)
+    if scratch_limit:
+        renderer.set_scratch_limit(scratch_limit)
+    prepared = renderer.prepare(plans)
+    prepared.run()
+    pcm, results = prepared.collect()
+    mix = prepared.mix()
+    segments = prepared.segments
+    prepared.close()
+    renderer.close()
+    return mix, pcm, results, segments
+
+
+def compare_pcm(pcm, expected):
+    assert pcm.shape == expected.shape
+    diff = np.abs(pcm.astype(np.int32) - expected.astype(np.int32))
+    identical = float(np.mean(diff == 0)) if diff.size else 1.0
+    assert diff.max(initial=0) <= 1, f"PCM16 differs by {diff.max()} LSB"
+    assert identical >= PCM_IDENTICAL, f"only {identical:.5f} of PCM16 samples identical"
+    return identical
+
+
+def compare_results(results, expected):
+    for field in ("status", "frames", "dataFrames", "fade", "offset"):
+        np.testing.assert_array_equal(results[field], expected[field], err_msg=field)
+
+
+def plan_jobs(session, jobs, tail="natural"):
+    return [session.plan(j.sfz, j.midi, tail=tail) for j in jobs]
+
+
+@pytest.mark.parametrize("tail", ["natural", "orig"])
+def test_plain_small_matches_reference(plain_small, ref_session, tail):
+    from oracle import oracle, reference
+    plans = plan_jobs(ref_session, plain_small, tail)
+    bank = ref_session.bank()
+    natural = tail == "natural"
+    mix, pcm, results, _ = render(plans, bank, natural)
+    ref_mix = reference.synthesize(plans, bank, natural)
+    if natural:
+        err = float(np.max(np.abs(mix - ref_mix)))
+        assert err <= BUS_TOLERANCE, err
+    else:
+        assert np.max(np.abs(mix.astype(np.int32) - ref_mix.astype(np.int32))) <= 1
+    ref_pcm, ref_results = oracle.finish(ref_mix, plans, natural)
+    compare_results(results, ref_results)
+    compare_pcm(pcm, ref_pcm)
+
+
+@pytest.mark.parametrize("tail", ["natural", "orig"])
+def test_filtered_batch_matches_reference(batch_mini, ref_session, tail):
+    from oracle import oracle, reference
+    plans = plan_jobs(ref_session, batch_mini, tail)
+    assert all(p.filter_tracks > 0 for p in plans)
+    bank = ref_session.bank()
+    natural = tail == "natural"
+    mix, pcm, results, _ = render(plans, bank, natural)
+    ref_mix = reference.synthesize(plans, bank, natural)
+    if natural:
+        err = float(np.max(np.abs(mix - ref_mix)))
+        assert err <= BUS_TOLERANCE, err
+    else:
+        assert np.max(np.abs(mix.astype(np.int32) - ref_mix.astype(np.int32))) <= 1
+    ref_pcm, ref_results = oracle.finish(ref_mix, plans, natural)
+    compare_results(results, ref_results)
+    compare_pcm(pcm, ref_pcm)
+
+
+def test_segmented_synthesis_is_byte_identical(batch_mini, ref_session):
+    """Chain state (filter history, smoothing, loop phase) carries across segments."""
+    plans = plan_jobs(ref_session, batch_mini)
+    bank = ref_session.bank()
+    mix, pcm, results, segments = render(plans, bank)
+    mix2, pcm2, results2, segments2 = render(plans, bank, scratch_limit=64 * 1024)
+    assert segments == 1 and segments2 > 4
+    assert np.array_equal(mix.view(np.uint32), mix2.view(np.uint32))
+    assert np.array_equal(pcm, pcm2)
+    assert results.tobytes() == results2.tobytes()
