@@ -238,6 +238,561 @@ __global__ void __launch_bounds__(kChainWarps * 32) chainKernel(BatchView b, Seg
     }
 }
 
+// ---- single-slot chains: parallel sources, one recurrence per lane -------------------
+//
+// Chains whose spans all filter through one main slot with one filter type run in
+// two kernels.  sourceKernel renders every voice frame in parallel (one thread per
+// frame, 256-frame tiles) and, for moving filters, the per-frame target
+// coefficients in a 3-float form: for the low/high/band-pass, notch and one-pole
+// designs the remaining coefficients are exact multiples (x2, -1, equal) of these
+// three, and the component-wise smoothing preserves those relations bit for bit.
+// recurrenceKernel then runs each chain's smoothing and biquad cascade serially in
+// one lane, streaming four frames per step with 128-bit loads.
+
+__device__ __forceinline__ int activeSlot(const cs_voice_span& v)
+{
+    for (int f = 0; f < 2; ++f)
+        if (v.filters[f].type != CS_FILTER_NONE)
+            return f;
+    return -1;
+}
+
+struct Compact {
+    float c0, c1, c2;
+};
+
+__device__ __forceinline__ Compact compactOf(int type, const Biquad& q)
+{
+    (void)type;
+    return {q.b0, q.a1, q.a2};
+}
+
+__device__ __forceinline__ Biquad expand(int type, const Compact& c)
+{
+    switch (type) {
+    case CS_FILTER_LOW1: return {c.c0, 0.f, 0.f, c.c1, 0.f};
+    case CS_FILTER_HIGH1: return {c.c0, -c.c0, 0.f, c.c1, 0.f};
+    case CS_FILTER_HIGH2: case CS_FILTER_HIGH4: case CS_FILTER_HIGH6:
+        return {c.c0, -2 * c.c0, c.c0, c.c1, c.c2};
+    case CS_FILTER_BAND2: case CS_FILTER_BAND4: case CS_FILTER_BAND6:
+        return {c.c0, 0.f, -c.c0, c.c1, c.c2};
+    case CS_FILTER_NOTCH2: return {c.c0, c.c1, c.c0, c.c1, c.c2};
+    default: return {c.c0, 2 * c.c0, c.c0, c.c1, c.c2};
+    }
+}
+
+__global__ void __launch_bounds__(kSourceTile) sourceKernel(BatchView b, SegmentView s)
+{
+    const int2 tile = s.sourceTiles[blockIdx.x];
+    const int span = tile.x;
+    const cs_voice_span& v = b.voices[span];
+    const int frame = tile.y + int(threadIdx.x);
+    const int start = max(v.begin, s.first), stop = min(v.end, s.end);
+    if (frame >= stop)
+        return;
+    const double position = v.variablePitch ? b.phase[s.phaseOffset[span] + (frame - start)] : -1.0;
+    const int* tracks = v.filterControls;
+    const float pan = trackAt(b.points, tracks[2], tracks[3], frame);
+    const float2 sample = voiceFrame(b.bank, b.sinc, v, b.points, b.modulation, pan, frame, true, position);
+    const float gain = jobGainAt(b.points, tracks, frame);
+    float* dst = b.filtered + s.scratchOffset[span] + size_t(frame - start) * v.channels;
+    dst[0] = sample.x * gain;
+    if (v.channels == 2)
+        dst[1] = sample.y * gain;
+    const uint64_t targets = s.targetOffset[span];
+    if (targets == kNoTargets)
+        return;
+    const bool moving = filterMoves(v, b.modulation);
+    if (!moving && frame != v.begin)
+        return;
+    const int f = activeSlot(v);
+    const Compact c = compactOf(v.filters[f].type, filterTargetSlot(v, b.points, b.modulation, frame, f));
+    if (moving) {
+        const int rel = frame - start;
+        float* out = b.filtered + targets + size_t(rel / kRecChunkFrames) * 3 * kRecChunkFrames + rel % kRecChunkFrames;
+        out[0] = c.c0;
+        out[kRecChunkFrames] = c.c1;
+        out[2 * kRecChunkFrames] = c.c2;
+    } else {
+        float* out = b.filtered + targets;
+        out[0] = c.c0;
+        out[1] = c.c1;
+        out[2] = c.c2;
+    }
+}
+
+struct RecurrenceState {
+    Compact c;
+    float z1l[3], z2l[3], z1r[3], z2r[3];
+};
+
+template <bool Stereo>
+__device__ __forceinline__ void cascade(float& x, float& y, const Biquad& q, int sections, RecurrenceState& st)
+{
+    #pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (k < sections) {
+            x = biquadStep(x, q, st.z1l[k], st.z2l[k]);
+            if (Stereo)
+                y = biquadStep(y, q, st.z1r[k], st.z2r[k]);
+        }
+    }
+}
+
+// One span of one chain: smoothing + cascade over frames [0, n) in place.
+template <bool Stereo>
+__device__ __forceinline__ void runSpan(float* src, const float* tgt, int n, int type, int sections, bool moving,
+                                        float amount, bool& initialized, RecurrenceState& st)
+{
+    constexpr int ch = Stereo ? 2 : 1;
+    const auto step = [&](float& x, float& y, float t0, float t1, float t2, bool haveTarget) {
+        if (haveTarget) {
+            if (initialized) {
+                st.c.c0 = fmaf(amount, t0 - st.c.c0, st.c.c0);
+                st.c.c1 = fmaf(amount, t1 - st.c.c1, st.c.c1);
+                st.c.c2 = fmaf(amount, t2 - st.c.c2, st.c.c2);
+            } else {
+                st.c = {t0, t1, t2};
+            }
+        }
+        initialized = true;
+        const Biquad q = expand(type, st.c);
+        cascade<Stereo>(x, y, q, sections, st);
+    };
+    int i = 0;
+    if (moving && sections) {
+        for (; i + 4 <= n; i += 4) {
+            float xs[4], ys[4];
+            if (Stereo) {
+                const float4 a = *reinterpret_cast<const float4*>(src + 2 * i);
+                const float4 c = *reinterpret_cast<const float4*>(src + 2 * i + 4);
+                xs[0] = a.x; ys[0] = a.y; xs[1] = a.z; ys[1] = a.w;
+                xs[2] = c.x; ys[2] = c.y; xs[3] = c.z; ys[3] = c.w;
+            } else {
+                const float4 a = *reinterpret_cast<const float4*>(src + i);
+                xs[0] = a.x; xs[1] = a.y; xs[2] = a.z; xs[3] = a.w;
+                ys[0] = ys[1] = ys[2] = ys[3] = 0.f;
+            }
+            const float4 t0 = *reinterpret_cast<const float4*>(tgt + 3 * i);
+            const float4 t1 = *reinterpret_cast<const float4*>(tgt + 3 * i + 4);
+            const float4 t2 = *reinterpret_cast<const float4*>(tgt + 3 * i + 8);
+            step(xs[0], ys[0], t0.x, t0.y, t0.z, true);
+            step(xs[1], ys[1], t0.w, t1.x, t1.y, true);
+            step(xs[2], ys[2], t1.z, t1.w, t2.x, true);
+            step(xs[3], ys[3], t2.y, t2.z, t2.w, true);
+            if (Stereo) {
+                *reinterpret_cast<float4*>(src + 2 * i) = make_float4(xs[0], ys[0], xs[1], ys[1]);
+                *reinterpret_cast<float4*>(src + 2 * i + 4) = make_float4(xs[2], ys[2], xs[3], ys[3]);
+            } else {
+                *reinterpret_cast<float4*>(src + i) = make_float4(xs[0], xs[1], xs[2], xs[3]);
+            }
+        }
+        for (; i < n; ++i) {
+            float x = src[ch * i], y = Stereo ? src[ch * i + 1] : 0.f;
+            step(x, y, tgt[3 * i], tgt[3 * i + 1], tgt[3 * i + 2], true);
+            src[ch * i] = x;
+            if (Stereo) src[ch * i + 1] = y;
+        }
+        return;
+    }
+    if (i < n && sections && !initialized) {
+        float x = src[0], y = Stereo ? src[1] : 0.f;
+        step(x, y, tgt[0], tgt[1], tgt[2], true);
+        src[0] = x;
+        if (Stereo) src[1] = y;
+        i = 1;
+    }
+    initialized = initialized || n > 0;
+    if (!sections)
+        return;
+    const Biquad q = expand(type, st.c);
+    for (; i < n && (i & 3); ++i) {
+        float x = src[ch * i], y = Stereo ? src[ch * i + 1] : 0.f;
+        cascade<Stereo>(x, y, q, sections, st);
+        src[ch * i] = x;
+        if (Stereo) src[ch * i + 1] = y;
+    }
+    for (; i + 4 <= n; i += 4) {
+        float xs[4], ys[4];
+        if (Stereo) {
+            const float4 a = *reinterpret_cast<const float4*>(src + 2 * i);
+            const float4 c = *reinterpret_cast<const float4*>(src + 2 * i + 4);
+            xs[0] = a.x; ys[0] = a.y; xs[1] = a.z; ys[1] = a.w;
+            xs[2] = c.x; ys[2] = c.y; xs[3] = c.z; ys[3] = c.w;
+        } else {
+            const float4 a = *reinterpret_cast<const float4*>(src + i);
+            xs[0] = a.x; xs[1] = a.y; xs[2] = a.z; xs[3] = a.w;
+            ys[0] = ys[1] = ys[2] = ys[3] = 0.f;
+        }
+        #pragma unroll
+        for (int k = 0; k < 4; ++k)
+            cascade<Stereo>(xs[k], ys[k], q, sections, st);
+        if (Stereo) {
+            *reinterpret_cast<float4*>(src + 2 * i) = make_float4(xs[0], ys[0], xs[1], ys[1]);
+            *reinterpret_cast<float4*>(src + 2 * i + 4) = make_float4(xs[2], ys[2], xs[3], ys[3]);
+        } else {
+            *reinterpret_cast<float4*>(src + i) = make_float4(xs[0], xs[1], xs[2], xs[3]);
+        }
+    }
+    for (; i < n; ++i) {
+        float x = src[ch * i], y = Stereo ? src[ch * i + 1] : 0.f;
+        cascade<Stereo>(x, y, q, sections, st);
+        src[ch * i] = x;
+        if (Stereo) src[ch * i + 1] = y;
+    }
+}
+
+// ---- TMA-staged serial recurrences --------------------------------------------------
+//
+// Lane = chain.  Each lane keeps two 32-frame chunks of its chain in shared memory,
+// filled by cp.async.bulk copies that complete on the lane's own mbarriers, so the
+// next chunk's sources and targets arrive while the current one runs through the
+// smoothing and biquad recurrence.  Waits are bounded: a wait that runs out sets
+// the batch's error flag and the lane stops.
+
+constexpr int kRecChunk = 32;
+constexpr int kRecBuffers = 3;
+constexpr int kRecBuffer = kRecChunk * 2 * 4 + kRecChunk * 3 * 4;     // 640 bytes: sources, targets
+constexpr int kRecChainBytes = kRecBuffers * kRecBuffer + 16;         // skew: conflict-free LDS.128
+constexpr int kRecChains = 16;                                        // per warp: lane = 2 * chain + channel
+constexpr int kRecWarps = 2;
+constexpr int kRecThreads = 32 * kRecWarps;
+constexpr long long kWaitLimit = 1ll << 24;
+
+__device__ __forceinline__ uint32_t sharedAddress(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void barrierInit(uint64_t* bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sharedAddress(bar)) : "memory");
+}
+
+__device__ __forceinline__ void barrierExpect(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sharedAddress(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulkLoad(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(sharedAddress(dst)), "l"(src), "r"(bytes), "r"(sharedAddress(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool barrierTryWait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                 " selp.u32 %0, 1, 0, p;\n}" : "=r"(done) : "r"(sharedAddress(bar)), "r"(parity) : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ bool barrierWait(uint64_t* bar, uint32_t parity)
+{
+    for (long long i = 0; i < kWaitLimit; ++i)
+        if (barrierTryWait(bar, parity))
+            return true;
+    return false;
+}
+
+__device__ __forceinline__ uint32_t round16(uint32_t bytes) { return (bytes + 15u) & ~15u; }
+
+struct ChainCursor {
+    int span, pos, stop, start;         // frames, job-local
+};
+
+__device__ __forceinline__ ChainCursor firstCursor(const cs_voice_span* voices, int from, const SegmentView& s)
+{
+    for (int at = from; at >= 0; at = voices[at].nextFilteredSpan) {
+        const cs_voice_span& v = voices[at];
+        if (v.begin >= s.end)
+            break;
+        if (v.end > s.first) {
+            const int start = max(v.begin, s.first);
+            return {at, start, min(v.end, s.end), start};
+        }
+    }
+    return {-1, 0, 0, 0};
+}
+
+__device__ __forceinline__ ChainCursor advanceCursor(const cs_voice_span* voices, ChainCursor c, const SegmentView& s)
+{
+    c.pos += min(kRecChunk, c.stop - c.pos);
+    if (c.pos < c.stop)
+        return c;
+    return firstCursor(voices, voices[c.span].nextFilteredSpan, s);
+}
+
+// One channel of one chain through staged frames [first, count) of a 32-frame
+// chunk.  Sources are interleaved per frame (stereo) and targets are planar, so
+// aligned groups of four frames need one or two 128-bit loads each; Type fixes
+// how the two derived numerator taps follow from the three carried coefficients.
+template <int Type, int Sections, bool Moving, bool Stereo>
+__device__ __forceinline__ void recurChunk(const float* __restrict__ frames, const float* __restrict__ targets,
+                                           float* __restrict__ out, int first, int count, int channel,
+                                           float amount, Compact& c, float* z1, float* z2)
+{
+    constexpr int stride = Stereo ? 2 : 1;
+    const auto frameStep = [&](float x, float t0, float t1, float t2) {
+        if (Moving) {
+            c.c0 = fmaf(amount, t0 - c.c0, c.c0);
+            c.c1 = fmaf(amount, t1 - c.c1, c.c1);
+            c.c2 = fmaf(amount, t2 - c.c2, c.c2);
+        }
+        const Biquad q = expand(Type, c);
+        #pragma unroll
+        for (int sct = 0; sct < Sections; ++sct)
+            x = biquadStep(x, q, z1[sct], z2[sct]);
+        return x;
+    };
+    int i = first;
+    for (; i < count && (i & 3); ++i) {
+        const float x = frames[stride * i + channel];
+        out[stride * i] = frameStep(x, Moving ? targets[i] : 0.f, Moving ? targets[kRecChunkFrames + i] : 0.f,
+                                    Moving ? targets[2 * kRecChunkFrames + i] : 0.f);
+    }
+    for (; i + 4 <= count; i += 4) {
+        float x[4];
+        if (Stereo) {
+            const float4 a = *reinterpret_cast<const float4*>(frames + 2 * i);
+            const float4 b2 = *reinterpret_cast<const float4*>(frames + 2 * i + 4);
+            x[0] = channel ? a.y : a.x;
+            x[1] = channel ? a.w : a.z;
+            x[2] = channel ? b2.y : b2.x;
+            x[3] = channel ? b2.w : b2.z;
+        } else {
+            const float4 a = *reinterpret_cast<const float4*>(frames + i);
+            x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+        }
+        float4 t0 = make_float4(0, 0, 0, 0), t1 = t0, t2 = t0;
+        if (Moving) {
+            t0 = *reinterpret_cast<const float4*>(targets + i);
+            t1 = *reinterpret_cast<const float4*>(targets + kRecChunkFrames + i);
+            t2 = *reinterpret_cast<const float4*>(targets + 2 * kRecChunkFrames + i);
+        }
+        out[stride * (i + 0)] = frameStep(x[0], t0.x, t1.x, t2.x);
+        out[stride * (i + 1)] = frameStep(x[1], t0.y, t1.y, t2.y);
+        out[stride * (i + 2)] = frameStep(x[2], t0.z, t1.z, t2.z);
+        out[stride * (i + 3)] = frameStep(x[3], t0.w, t1.w, t2.w);
+    }
+    for (; i < count; ++i) {
+        const float x = frames[stride * i + channel];
+        out[stride * i] = frameStep(x, Moving ? targets[i] : 0.f, Moving ? targets[kRecChunkFrames + i] : 0.f,
+                                    Moving ? targets[2 * kRecChunkFrames + i] : 0.f);
+    }
+}
+
+template <int Type, bool Stereo>
+__device__ __forceinline__ void recurSections(const float* frames, const float* targets, float* out, int first,
+                                              int count, int channel, int sections, bool moving, float amount,
+                                              Compact& c, float* z1, float* z2)
+{
+    if (moving) {
+        if (sections == 1) recurChunk<Type, 1, true, Stereo>(frames, targets, out, first, count, channel, amount, c, z1, z2);
+        else if (sections == 2) recurChunk<Type, 2, true, Stereo>(frames, targets, out, first, count, channel, amount, c, z1, z2);
+        else recurChunk<Type, 3, true, Stereo>(frames, targets, out, first, count, channel, amount, c, z1, z2);
+    } else {
+        if (sections == 1) recurChunk<Type, 1, false, Stereo>(frames, targets, out, first, count, channel, amount, c, z1, z2);
+        else if (sections == 2) recurChunk<Type, 2, false, Stereo>(frames, targets, out, first, count, channel, amount, c, z1, z2);
+        else recurChunk<Type, 3, false, Stereo>(frames, targets, out, first, count, channel, amount, c, z1, z2);
+    }
+}
+
+template <bool Stereo>
+__device__ __forceinline__ void recurDispatch(int type, const float* frames, const float* targets, float* out,
+                                              int first, int count, int channel, int sections, bool moving,
+                                              float amount, Compact& c, float* z1, float* z2)
+{
+    switch (type) {
+    case CS_FILTER_LOW1:
+        recurSections<CS_FILTER_LOW1, Stereo>(frames, targets, out, first, count, channel, sections, moving, amount, c, z1, z2);
+        break;
+    case CS_FILTER_HIGH1:
+        recurSections<CS_FILTER_HIGH1, Stereo>(frames, targets, out, first, count, channel, sections, moving, amount, c, z1, z2);
+        break;
+    case CS_FILTER_HIGH2: case CS_FILTER_HIGH4: case CS_FILTER_HIGH6:
+        recurSections<CS_FILTER_HIGH2, Stereo>(frames, targets, out, first, count, channel, sections, moving, amount, c, z1, z2);
+        break;
+    case CS_FILTER_BAND2: case CS_FILTER_BAND4: case CS_FILTER_BAND6:
+        recurSections<CS_FILTER_BAND2, Stereo>(frames, targets, out, first, count, channel, sections, moving, amount, c, z1, z2);
+        break;
+    case CS_FILTER_NOTCH2:
+        recurSections<CS_FILTER_NOTCH2, Stereo>(frames, targets, out, first, count, channel, sections, moving, amount, c, z1, z2);
+        break;
+    default:
+        recurSections<CS_FILTER_LOW2, Stereo>(frames, targets, out, first, count, channel, sections, moving, amount, c, z1, z2);
+        break;
+    }
+}
+
+// Per-span constants of a chain cursor, loaded once when the cursor enters a span.
+struct SpanRun {
+    int span, pos, stop, start, channels, sections;
+    int moving;
+    float amount;
+    const float* src;                   // span's source frames in the segment scratch
+    const float* tgt;                   // span's filter targets (moving: per frame)
+};
+
+__device__ __forceinline__ SpanRun enterRun(const BatchView& b, const SegmentView& s, int from, int fslot)
+{
+    const cs_voice_span* voices = b.voices;
+    for (int at = from; at >= 0; at = voices[at].nextFilteredSpan) {
+        const cs_voice_span& v = voices[at];
+        if (v.begin >= s.end)
+            break;
+        if (v.end <= s.first)
+            continue;
+        SpanRun r;
+        r.span = at;
+        r.start = max(v.begin, s.first);
+        r.pos = r.start;
+        r.stop = min(v.end, s.end);
+        r.channels = v.channels;
+        r.sections = filterSections(v.filters[fslot].type);
+        const uint64_t toff = s.targetOffset[at];
+        r.moving = toff != kNoTargets && filterMoves(v, b.modulation);
+        r.amount = 1 - expf(-1000.f / float(v.sampleRate));
+        r.src = b.filtered + s.scratchOffset[at];
+        r.tgt = b.filtered + (toff == kNoTargets ? 0 : toff);
+        return r;
+    }
+    SpanRun none{};
+    none.span = -1;
+    return none;
+}
+
+__device__ __forceinline__ void advanceRun(const BatchView& b, const SegmentView& s, SpanRun& r, int fslot)
+{
+    r.pos += min(kRecChunk, r.stop - r.pos);
+    if (r.pos >= r.stop)
+        r = enterRun(b, s, b.voices[r.span].nextFilteredSpan, fslot);
+}
+
+__global__ void __launch_bounds__(kRecThreads) recurrenceKernel(BatchView b, SegmentView s, int* error)
+{
+    extern __shared__ __align__(16) unsigned char staged[];
+    __shared__ __align__(8) uint64_t bars[kRecWarps * kRecChains][kRecBuffers];
+    const int lane = int(threadIdx.x & 31), warp = int(threadIdx.x >> 5);
+    const int local = warp * kRecChains + (lane >> 1);
+    const int channel = lane & 1;
+    const int chain = int(blockIdx.x) * kRecWarps * kRecChains + local;
+    const cs_voice_span* voices = b.voices;
+    int head = -1, fslot = -1, type = CS_FILTER_NONE;
+    if (chain < s.simpleCount) {
+        head = s.simple[chain];
+        fslot = activeSlot(voices[head]);
+        if (fslot >= 0)
+            type = voices[head].filters[fslot].type;
+    }
+    // Pitch-only chains and mono chains' right lanes have nothing to run.
+    const bool leader = channel == 0 && fslot >= 0;
+    const bool active = fslot >= 0 && (channel == 0 || voices[head].channels == 2);
+    unsigned char* region = staged + size_t(local) * kRecChainBytes;
+    if (leader)
+        for (int k = 0; k < kRecBuffers; ++k)
+            barrierInit(&bars[local][k]);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncwarp();
+    if (!active)
+        return;
+    // Both lanes of a stereo chain read each staged buffer before it is refilled.
+    const unsigned pair = (voices[head].channels == 2 ? 3u : 1u) << (lane & ~1);
+    ChainState& state = b.states[head];
+    bool initialized = state.filterInitialized != 0;
+    Compact c{state.coefficients[fslot][0], state.coefficients[fslot][3], state.coefficients[fslot][4]};
+    float z1[3], z2[3];
+    #pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        z1[k] = state.z1[fslot][k][channel];
+        z2[k] = state.z2[fslot][k][channel];
+    }
+
+    SpanRun consume = enterRun(b, s, head, fslot);
+    SpanRun next = consume;
+    const auto issue = [&](int slot) {
+        const int count = min(kRecChunk, next.stop - next.pos);
+        const int rel = next.pos - next.start;
+        const uint32_t srcBytes = round16(uint32_t(count * next.channels) * 4u);
+        const uint32_t tgtBytes = next.moving ? uint32_t(3 * kRecChunkFrames * 4) : 0u;
+        unsigned char* buffer = region + slot * kRecBuffer;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        barrierExpect(&bars[local][slot], srcBytes + tgtBytes);
+        bulkLoad(buffer, next.src + size_t(rel) * next.channels, srcBytes, &bars[local][slot]);
+        if (tgtBytes)
+            bulkLoad(buffer + kRecChunk * 2 * 4, next.tgt + size_t(rel / kRecChunk) * 3 * kRecChunk, tgtBytes,
+                     &bars[local][slot]);
+    };
+    uint32_t phases = 0;                 // bit k: parity of buffer k's next completion
+    for (int slot = 0; slot < kRecBuffers && next.span >= 0; ++slot) {
+        if (leader)
+            issue(slot);
+        advanceRun(b, s, next, fslot);
+    }
+    int slot = 0;
+    while (consume.span >= 0) {
+        if (!barrierWait(&bars[local][slot], (phases >> slot) & 1u)) {
+            atomicExch(error, 1);
+            return;
+        }
+        phases ^= 1u << slot;
+        const int count = min(kRecChunk, consume.stop - consume.pos);
+        const int rel = consume.pos - consume.start;
+        const int sections = consume.sections;
+        const bool moving = consume.moving != 0;
+        const int stride = consume.channels;
+        const float* frames = reinterpret_cast<const float*>(region + slot * kRecBuffer);
+        const float* targets = frames + kRecChunk * 2;
+        float* out = const_cast<float*>(consume.src) + size_t(rel) * stride + channel;
+        if (sections) {
+            int first = 0;
+            if (!initialized) {
+                // The chain's first frame takes its targets without smoothing.
+                if (moving)
+                    c = {targets[0], targets[kRecChunk], targets[2 * kRecChunk]};
+                else
+                    c = {consume.tgt[0], consume.tgt[1], consume.tgt[2]};
+                initialized = true;
+                const Biquad q = expand(type, c);
+                float x = frames[channel];
+                for (int k = 0; k < sections; ++k)
+                    x = biquadStep(x, q, z1[k], z2[k]);
+                out[0] = x;
+                first = 1;
+            }
+            if (stride == 2)
+                recurDispatch<true>(type, frames, targets, out, first, count, channel, sections, moving,
+                                    consume.amount, c, z1, z2);
+            else
+                recurDispatch<false>(type, frames, targets, out, first, count, channel, sections, moving,
+                                     consume.amount, c, z1, z2);
+        } else {
+            initialized = true;
+        }
+        advanceRun(b, s, consume, fslot);
+        __syncwarp(pair);
+        if (next.span >= 0) {
+            if (leader)
+                issue(slot);
+            advanceRun(b, s, next, fslot);
+        }
+        slot = slot + 1 == kRecBuffers ? 0 : slot + 1;
+    }
+    if (channel == 0) {
+        state.filterInitialized = initialized;
+        const Biquad q = expand(type, c);
+        float* coeff = state.coefficients[fslot];
+        coeff[0] = q.b0; coeff[1] = q.b1; coeff[2] = q.b2; coeff[3] = q.a1; coeff[4] = q.a2;
+    }
+    #pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        state.z1[fslot][k][channel] = z1[k];
+        state.z2[fslot][k][channel] = z2[k];
+    }
+}
+
 // ---- mix + block scan ----------------------------------------------------------------
 
 constexpr int kMixThreads = 256;
@@ -592,11 +1147,30 @@ void launchPitch(const BatchView& b, const SegmentView& s, cudaStream_t stream)
     pitchKernel<<<(s.pitchCount + 63) / 64, 64, 0, stream>>>(b, s);
 }
 
-void launchChains(const BatchView& b, const SegmentView& s, cudaStream_t stream)
+int launchChains(const BatchView& b, const SegmentView& s, cudaStream_t stream)
 {
-    if (!s.chainCount)
-        return;
-    chainKernel<<<(s.chainCount + kChainWarps - 1) / kChainWarps, kChainWarps * 32, 0, stream>>>(b, s);
+    int launches = 0;
+    if (s.sourceTileCount) {
+        sourceKernel<<<s.sourceTileCount, kSourceTile, 0, stream>>>(b, s);
+        ++launches;
+    }
+    if (s.simpleCount) {
+        constexpr int chainsPerCta = kRecWarps * kRecChains;
+        constexpr int bytes = chainsPerCta * kRecChainBytes;
+        static bool configured = false;
+        if (!configured) {
+            cudaFuncSetAttribute(recurrenceKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            configured = true;
+        }
+        recurrenceKernel<<<(s.simpleCount + chainsPerCta - 1) / chainsPerCta, kRecThreads, bytes, stream>>>(
+            b, s, b.error);
+        ++launches;
+    }
+    if (s.chainCount) {
+        chainKernel<<<(s.chainCount + kChainWarps - 1) / kChainWarps, kChainWarps * 32, 0, stream>>>(b, s);
+        ++launches;
+    }
+    return launches;
 }
 
 void launchMix(const BatchView& b, const SegmentView& s, bool natural, StereoStats* stats, cudaStream_t stream)

@@ -12,6 +12,11 @@ constexpr int kPhases = 2048;           // render.cu:4
 constexpr int kTileFrames = 256;       // frames per mix tile (one voice list each)
 constexpr int kBlockFrames = CS_TAIL_BLOCK_FRAMES;
 constexpr int kTilesPerBlock = kBlockFrames / kTileFrames;
+constexpr int kSourceTile = 256;         // frames per source-kernel CTA
+constexpr uint64_t kNoTargets = ~uint64_t(0);
+// Moving-filter targets are stored per 32-frame chunk as three planes
+// (c0[32], c1[32], c2[32]) so the recurrence reads four frames per 128-bit load.
+constexpr int kRecChunkFrames = 32;
 
 // A mix tile: kTileFrames frames of one job with the spans that overlap it
 // (the reference's Tile, src/cuda/render_types.h:70-74).
@@ -61,6 +66,7 @@ struct BatchView {
     float* filtered;
     double* phase;
     void* mix;                          // float2 (natural) or short2
+    int* error;                         // set by kernels whose bounded waits ran out
     int jobCount;
 };
 
@@ -68,8 +74,13 @@ struct SegmentView {
     int first, end;                     // job-local frame range, 1024-aligned
     const uint64_t* scratchOffset;      // per voice: float offset into `filtered`
     const uint64_t* phaseOffset;        // per voice: offset into `phase`
-    const int* chains;                  // heads of chains active in this segment
+    const int* chains;                  // heads of general chains active in this segment
     int chainCount;
+    const int* simple;                  // heads of single-slot chains, longest first
+    int simpleCount;
+    const uint64_t* targetOffset;       // per voice: float offset of its filter targets
+    const int2* sourceTiles;            // (span, first frame) of 256-frame source tiles
+    int sourceTileCount;
     const int* pitchChains;
     int pitchCount;
     const int* blocks;                  // mix blocks in this segment
@@ -88,7 +99,7 @@ struct FinishView {
 void buildSincTable(float* phaseMajor);   // host: 2049 x 48 floats
 
 void launchPitch(const BatchView& b, const SegmentView& s, cudaStream_t stream);
-void launchChains(const BatchView& b, const SegmentView& s, cudaStream_t stream);
+int launchChains(const BatchView& b, const SegmentView& s, cudaStream_t stream);
 void launchMix(const BatchView& b, const SegmentView& s, bool natural, StereoStats* stats, cudaStream_t stream);
 int launchFinish(const BatchView& b, const FinishView& f, bool natural, bool quality, const TailConfig& tail,
                  cudaStream_t stream);

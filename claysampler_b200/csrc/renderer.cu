@@ -158,34 +158,108 @@ struct HostBatch {
 struct SegmentPlan {
     int first, end;
     size_t scratchFloats, phaseFrames;
-    size_t chainFirst, chainCount, pitchFirst, pitchCount, blockFirst, blockCount;
+    size_t chainFirst, chainCount, simpleFirst, simpleCount, pitchFirst, pitchCount, blockFirst, blockCount;
+    size_t tileFirst, tileCount;
 };
 
 // Host side of a staged batch: segment boundaries and the per-segment arrays.
 struct SegmentTables {
     std::vector<SegmentPlan> segments;
-    std::vector<uint64_t> scratchOffset, phaseOffset;   // segments x voices
-    std::vector<int> chains, pitch, blocks;
+    std::vector<uint64_t> scratchOffset, phaseOffset, targetOffset;   // segments x voices
+    std::vector<int> chains, simple, pitch, blocks;
+    std::vector<int2> tiles;
     size_t scratchBytes = 0;
 };
 
+// A chain runs on the one-recurrence-per-lane kernel when every span filters
+// through at most one of the two main slots, and always the same one.
+bool singleSlotChain(const HostBatch& batch, int head)
+{
+    int slot = -1, type = CS_FILTER_NONE;
+    for (int span = head; span >= 0; span = batch.voices[size_t(span)].nextFilteredSpan) {
+        const auto& v = batch.voices[size_t(span)];
+        int spanSlot = -1;
+        for (int f = 0; f < CS_FILTER_SLOTS; ++f) {
+            if (v.filters[f].type == CS_FILTER_NONE)
+                continue;
+            if (f >= 2 || spanSlot >= 0)
+                return false;
+            spanSlot = f;
+        }
+        if (spanSlot >= 0) {
+            if (slot >= 0 && (slot != spanSlot || v.filters[spanSlot].type != type))
+                return false;
+            slot = spanSlot;
+            type = v.filters[spanSlot].type;
+            if (type == CS_FILTER_PEAK)
+                return false;
+        }
+    }
+    return true;
+}
+
+// filterMoves (render.cu:370-375) on the host.
+bool spanMoves(const HostBatch& batch, const cs_voice_span& v)
+{
+    bool moving = v.activeEnvelope[0] != 0;
+    for (int j = v.firstModulation; j < v.firstModulation + v.modulationCount; ++j) {
+        const int target = batch.modulation[size_t(j)].target;
+        moving |= (target >= CS_MOD_CUTOFF && target <= CS_MOD_RESONANCE2) || target == CS_MOD_FILEG_DEPTH ||
+            target >= CS_MOD_EQ1_FREQUENCY;
+    }
+    return moving;
+}
+
 size_t scratchBytesOf(size_t floats, size_t phases) { return align256(floats * sizeof(float)) + phases * sizeof(double); }
 
+size_t alignFloats(size_t floats) { return (floats + 3) & ~size_t(3); }
+
 // Cuts [0, lastFrame) at 1024-frame boundaries so that each segment's chain
-// storage fits `budget` (one block per segment at least).
+// storage fits `budget` (one block per segment at least), then lays out every
+// segment's storage: per span its source frames (16-byte aligned) and, for
+// single-slot chains, its filter targets (every frame when the filter moves, the
+// first frame of the chain otherwise).
 SegmentTables planSegments(const HostBatch& batch, size_t budget)
 {
     SegmentTables t;
+    const size_t voiceCount = batch.voices.size();
+    // Chain membership and kind of every chain span.
+    std::vector<int> chainOf(voiceCount, -1);
+    std::vector<char> simple(voiceCount, 0), moving(voiceCount, 0), head(voiceCount, 0);
+    for (int h : batch.chainHeads) {
+        const bool single = singleSlotChain(batch, h);
+        head[size_t(h)] = 1;
+        for (int span = h; span >= 0; span = batch.voices[size_t(span)].nextFilteredSpan) {
+            chainOf[size_t(span)] = h;
+            simple[size_t(span)] = single;
+            moving[size_t(span)] = spanMoves(batch, batch.voices[size_t(span)]);
+        }
+    }
+    const auto hasFilter = [&](const cs_voice_span& v) {
+        for (const auto& f : v.filters)
+            if (f.type != CS_FILTER_NONE)
+                return true;
+        return false;
+    };
+    const auto targetFloats = [&](size_t v, int frames) -> size_t {
+        if (!simple[v] || !hasFilter(batch.voices[v]))
+            return 0;
+        if (moving[v])
+            return size_t((frames + kRecChunkFrames - 1) / kRecChunkFrames) * 3 * kRecChunkFrames;
+        return head[v] ? 4 : 0;
+    };
     const int lastFrame = batch.lastFrame;
     const int blocks = (lastFrame + kBlockFrames - 1) / kBlockFrames;
-    // Per-block storage demand of every chain span, via a difference array.
+    // Per-block storage demand, via spans' block overlaps (slack for alignment).
     std::vector<long long> floatsPerBlock(size_t(blocks) + 1, 0), phasesPerBlock(size_t(blocks) + 1, 0);
-    for (const auto& v : batch.voices) {
+    for (size_t vi = 0; vi < voiceCount; ++vi) {
+        const auto& v = batch.voices[vi];
         if (v.filterTrack < 0)
             continue;
         for (int b = v.begin / kBlockFrames; b <= (v.end - 1) / kBlockFrames; ++b) {
             const int lo = std::max(v.begin, b * kBlockFrames), hi = std::min(v.end, (b + 1) * kBlockFrames);
-            floatsPerBlock[size_t(b)] += (long long)(hi - lo) * v.channels;
+            floatsPerBlock[size_t(b)] += (long long)(hi - lo) * v.channels + 8 +
+                (long long)targetFloats(vi, hi - lo);
             if (v.variablePitch)
                 phasesPerBlock[size_t(b)] += hi - lo;
         }
@@ -208,14 +282,15 @@ SegmentTables planSegments(const HostBatch& batch, size_t budget)
     }
     if (ranges.empty())
         ranges.emplace_back(0, 0);
-    const size_t voiceCount = batch.voices.size();
     t.scratchOffset.assign(voiceCount * ranges.size(), 0);
     t.phaseOffset.assign(voiceCount * ranges.size(), 0);
+    t.targetOffset.assign(voiceCount * ranges.size(), kNoTargets);
     for (size_t si = 0; si < ranges.size(); ++si) {
         SegmentPlan seg{};
         seg.first = ranges[si].first;
         seg.end = ranges[si].second;
         size_t floats = 0, phases = 0;
+        std::vector<size_t> targetNeed(voiceCount, 0);
         for (size_t v = 0; v < voiceCount; ++v) {
             const auto& voice = batch.voices[v];
             if (voice.filterTrack < 0)
@@ -223,15 +298,23 @@ SegmentTables planSegments(const HostBatch& batch, size_t budget)
             const int frames = std::max(0, std::min(voice.end, seg.end) - std::max(voice.begin, seg.first));
             t.scratchOffset[si * voiceCount + v] = floats;
             t.phaseOffset[si * voiceCount + v] = phases;
-            floats += size_t(frames) * size_t(voice.channels);
+            floats = alignFloats(floats + size_t(frames) * size_t(voice.channels));
             if (voice.variablePitch)
                 phases += size_t(frames);
+            if (frames > 0)
+                targetNeed[v] = targetFloats(v, frames);
+        }
+        for (size_t v = 0; v < voiceCount; ++v) {
+            if (!targetNeed[v])
+                continue;
+            t.targetOffset[si * voiceCount + v] = floats;
+            floats += targetNeed[v];
         }
         seg.scratchFloats = floats;
         seg.phaseFrames = phases;
         t.scratchBytes = std::max(t.scratchBytes, scratchBytesOf(floats, phases));
-        const auto active = [&](int head) {
-            for (int span = head; span >= 0; span = batch.voices[size_t(span)].nextFilteredSpan) {
+        const auto active = [&](int h) {
+            for (int span = h; span >= 0; span = batch.voices[size_t(span)].nextFilteredSpan) {
                 const auto& v = batch.voices[size_t(span)];
                 if (v.begin >= seg.end)
                     break;
@@ -241,14 +324,38 @@ SegmentTables planSegments(const HostBatch& batch, size_t budget)
             return false;
         };
         seg.chainFirst = t.chains.size();
-        for (int head : batch.chainHeads)
-            if (active(head))
-                t.chains.push_back(head);
+        seg.tileFirst = t.tiles.size();
+        std::vector<std::pair<long long, int>> simpleChains;
+        for (int h : batch.chainHeads) {
+            if (!active(h))
+                continue;
+            if (!simple[size_t(h)]) {
+                t.chains.push_back(h);
+                continue;
+            }
+            long long frames = 0;
+            for (int span = h; span >= 0; span = batch.voices[size_t(span)].nextFilteredSpan) {
+                const auto& v = batch.voices[size_t(span)];
+                const int lo = std::max(v.begin, seg.first), hi = std::min(v.end, seg.end);
+                frames += std::max(0, hi - lo);
+                for (int f = lo; f < hi; f += kSourceTile)
+                    t.tiles.push_back(make_int2(span, f));
+            }
+            simpleChains.emplace_back(-frames, h);
+        }
         seg.chainCount = t.chains.size() - seg.chainFirst;
+        seg.tileCount = t.tiles.size() - seg.tileFirst;
+        // Longest recurrences first: neighbouring lanes then run similar lengths.
+        std::stable_sort(simpleChains.begin(), simpleChains.end(),
+                         [](const auto& x, const auto& y) { return x.first < y.first; });
+        seg.simpleFirst = t.simple.size();
+        for (const auto& item : simpleChains)
+            t.simple.push_back(item.second);
+        seg.simpleCount = t.simple.size() - seg.simpleFirst;
         seg.pitchFirst = t.pitch.size();
-        for (int head : batch.pitchHeads)
-            if (active(head))
-                t.pitch.push_back(head);
+        for (int h : batch.pitchHeads)
+            if (active(h))
+                t.pitch.push_back(h);
         seg.pitchCount = t.pitch.size() - seg.pitchFirst;
         seg.blockFirst = t.blocks.size();
         for (const auto& job : batch.jobs) {
@@ -347,7 +454,10 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count)
     const size_t oWindowJob = section(batch.windowJob.size() * sizeof(int));
     const size_t oScratchOff = section(t.scratchOffset.size() * sizeof(uint64_t));
     const size_t oPhaseOff = section(t.phaseOffset.size() * sizeof(uint64_t));
+    const size_t oTargetOff = section(t.targetOffset.size() * sizeof(uint64_t));
+    const size_t oSourceTiles = section(t.tiles.size() * sizeof(int2));
     const size_t oChains = section(t.chains.size() * sizeof(int));
+    const size_t oSimple = section(t.simple.size() * sizeof(int));
     const size_t oPitch = section(t.pitch.size() * sizeof(int));
     const size_t oBlocks = section(t.blocks.size() * sizeof(int));
     const size_t uploadEnd = layout.bytes;
@@ -362,6 +472,7 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count)
     const size_t oMono = section(r.natural ? batch.frames * sizeof(short) : 0);
     const size_t oPacked = section(batch.frames * size_t(channels) * sizeof(short));
     const size_t oScratch = section(t.scratchBytes);
+    const size_t oError = section(sizeof(int));
     p->arenaBytes = layout.bytes;
 
     cudaError_t status = cudaMalloc(&p->arena, p->arenaBytes);
@@ -388,7 +499,10 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count)
     stage(oWindowJob, batch.windowJob);
     stage(oScratchOff, t.scratchOffset);
     stage(oPhaseOff, t.phaseOffset);
+    stage(oTargetOff, t.targetOffset);
+    stage(oSourceTiles, t.tiles);
     stage(oChains, t.chains);
+    stage(oSimple, t.simple);
     stage(oPitch, t.pitch);
     stage(oBlocks, t.blocks);
     check(cudaMemcpyAsync(base, staging.data(), uploadEnd, cudaMemcpyHostToDevice, r.stream), "CUDA batch upload");
@@ -408,6 +522,7 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count)
     v.states = reinterpret_cast<ChainState*>(base + oStates);
     v.filtered = reinterpret_cast<float*>(base + oScratch);
     v.mix = base + oMix;
+    v.error = reinterpret_cast<int*>(base + oError);
     v.jobCount = int(jobs);
     const size_t voiceCount = batch.voices.size();
     for (const auto& seg : t.segments) {
@@ -419,6 +534,11 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count)
         s.phaseOffset = reinterpret_cast<const uint64_t*>(base + oPhaseOff) + si * voiceCount;
         s.chains = reinterpret_cast<const int*>(base + oChains) + seg.chainFirst;
         s.chainCount = int(seg.chainCount);
+        s.simple = reinterpret_cast<const int*>(base + oSimple) + seg.simpleFirst;
+        s.simpleCount = int(seg.simpleCount);
+        s.targetOffset = reinterpret_cast<const uint64_t*>(base + oTargetOff) + si * voiceCount;
+        s.sourceTiles = reinterpret_cast<const int2*>(base + oSourceTiles) + seg.tileFirst;
+        s.sourceTileCount = int(seg.tileCount);
         s.pitchChains = reinterpret_cast<const int*>(base + oPitch) + seg.pitchFirst;
         s.pitchCount = int(seg.pitchCount);
         s.blocks = reinterpret_cast<const int*>(base + oBlocks) + seg.blockFirst;
@@ -452,6 +572,7 @@ void run(cs_renderer& r, cs_prepared& p, cudaStream_t stream)
     check(cudaEventRecord(p.begin, stream), "CUDA timing record");
     check(cudaMemsetAsync(p.view.states, 0, std::max<size_t>(p.stateBytes, 1), stream), "CUDA state reset");
     check(cudaMemsetAsync(p.finish.results, 0, std::max<size_t>(p.resultBytes, 1), stream), "CUDA result reset");
+    check(cudaMemsetAsync(p.view.error, 0, sizeof(int), stream), "CUDA error flag reset");
     for (size_t i = 0; i < p.segments.size(); ++i) {
         BatchView view = p.view;
         const SegmentPlan& plan = p.tables.segments[i];
@@ -459,9 +580,9 @@ void run(cs_renderer& r, cs_prepared& p, cudaStream_t stream)
                                                align256(plan.scratchFloats * sizeof(float)));
         const SegmentView& s = p.segments[i];
         launchPitch(view, s, stream);
-        launchChains(view, s, stream);
+        launches += launchChains(view, s, stream);
         launchMix(view, s, r.natural, p.stereo, stream);
-        launches += (s.pitchCount > 0) + (s.chainCount > 0) + (s.blockCount > 0);
+        launches += (s.pitchCount > 0) + (s.blockCount > 0);
     }
     check(cudaGetLastError(), "CUDA synthesis launch");
     launches += launchFinish(p.view, p.finish, r.natural, r.audio.enabled != 0, r.tail, stream);
@@ -475,6 +596,10 @@ void run(cs_renderer& r, cs_prepared& p, cudaStream_t stream)
 size_t collectResults(cs_renderer& r, cs_prepared& p)
 {
     check(cudaEventSynchronize(p.end), "CUDA render completion");
+    int failed = 0;
+    check(cudaMemcpy(&failed, p.view.error, sizeof(int), cudaMemcpyDeviceToHost), "CUDA error flag download");
+    if (failed)
+        throw std::runtime_error("a device wait ran out of its iteration limit (staged copy did not complete)");
     p.results.resize(p.batch.jobs.size());
     check(cudaMemcpy(p.results.data(), p.finish.results, p.resultBytes, cudaMemcpyDeviceToHost),
           "CUDA render metadata download");

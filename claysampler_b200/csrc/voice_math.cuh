@@ -359,3 +359,28 @@ __device__ __forceinline__ void filterTargets(const cs_voice_span& v, const cs_c
 }
 
 } // namespace cs
+
+namespace cs {
+
+// Target coefficients of one of the two main filter slots at `frame`; the same
+// accumulation as filterTargets restricted to slot `f` (render.cu:378-404).
+__device__ __forceinline__ Biquad filterTargetSlot(const cs_voice_span& v, const cs_control_point* __restrict__ points,
+                                                   const cs_voice_modulation* __restrict__ modulation, int frame, int f)
+{
+    float cents = 0, db = 0;
+    float depth = v.extraEnvelope[0].depth;
+    const int cutoffTarget = f == 0 ? CS_MOD_CUTOFF : CS_MOD_CUTOFF2;
+    const int resonanceTarget = f == 0 ? CS_MOD_RESONANCE : CS_MOD_RESONANCE2;
+    for (int j = v.firstModulation; j < v.firstModulation + v.modulationCount; ++j) {
+        const cs_voice_modulation m = modulation[j];
+        if (m.target == cutoffTarget) cents += bindingAt(m, points, frame);
+        else if (m.target == resonanceTarget) db += bindingAt(m, points, frame);
+        else if (f == 0 && m.target == CS_MOD_FILEG_DEPTH) depth += bindingAt(m, points, frame);
+    }
+    if (f == 0 && v.activeEnvelope[0])
+        cents += depth * envelopeAt(v.extraEnvelope[0], frame);
+    const cs_voice_filter& filter = v.filters[f];
+    return designFilter(filter.type, filter.cutoff * exp2f(cents / 1200), filter.resonance + db, v.sampleRate, 0, 0);
+}
+
+} // namespace cs
