@@ -1,0 +1,364 @@
+"""Throughput of the batch voice-render path: audio-seconds rendered per second.
+
+Workload (default): the 64-job plain batch — one preset of 88 keys x 4 velocity
+layers of stereo 24-bit samples (half looping), lpf_2p with a +-2400 cent filter
+envelope and a 5 Hz LFO on the cutoff, MIDI lengths log-uniform 10-180 s at
+Poisson 4 notes/s with sustain-pedal toggles — generated from a seed (the
+reference's sample libraries are not redistributable) and planned by this
+package's C++ host.
+
+A step renders the whole batch: synthesis (sources, filter recurrences, mix) and
+natural-tail finishing to packed mono PCM16.  `value` times steps on inputs that
+are already resident in device memory (bank 497 MB and per-step scratch well
+above the 126 MB L2, so no flush is needed); `e2e` times the public
+render_window call with the plans in host memory, including the plan upload and
+the PCM download.  Under torchrun every rank renders its own batch (no
+collective), so scaling is weak.
+
+`--impl reference` times the reference's own CPU implementation of the path
+(its src/cuda/render.cu built for the host, see oracle/ref) on a bounded sample
+of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+RATE = 44100
+METRIC = "audio-sec/sec on 1 B200 (batched+learned vs plain, ≤1 LSB); HBM GB/s; p99"
+WORKLOAD = "plain batch: 64 jobs, 88 keys x 4 layers stereo 24-bit, lpf_2p + fileg + 5 Hz LFO, loops, pedal"
+
+
+def parse():
+    p = argparse.ArgumentParser(description=__doc__)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    p.add_argument("--jobs", type=int, default=64)
+    p.add_argument("--seed", type=int, default=2)
+    p.add_argument("--cpu-sample-jobs", type=int, default=8)
+    p.add_argument("--workdir", type=Path, default=Path(tempfile.gettempdir()) / "claysampler_bench")
+    return p.parse_args()
+
+
+def dist_info():
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    return rank, world, local
+
+
+def workload(args, rank):
+    from claysampler_b200 import workload as wl
+    root = args.workdir / f"plain_batch_s{args.seed + rank}_j{args.jobs}"
+    marker = root / "ready"
+    if not marker.exists():
+        jobs = wl.write_plain_batch(root, seed=args.seed + rank, jobs=args.jobs)
+        marker.write_text("\n".join(f"{j.sfz}\t{j.midi}" for j in jobs))
+    return [tuple(map(Path, line.split("\t"))) for line in marker.read_text().splitlines()]
+
+
+def plan_jobs(jobs):
+    from claysampler_b200.host import Host
+    host = Host()
+    plans = [host.plan(sfz, midi, tail="natural") for sfz, midi in jobs]
+    bank = host.bank()
+    host.close()
+    return plans, bank
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.index)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, top, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                top = max(top, float(parts[1]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[3:7]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": top or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes(plans):
+    """Bytes each stage must move per launch (source samples read once at the voice's
+    step, scratch written/read once, mix written once), from the plans."""
+    src = rec = mix = 0.0
+    for p in plans:
+        s = p.spans
+        frames = (s["end"].astype(np.int64) - s["begin"]).astype(np.float64)
+        ch = s["channels"].astype(np.float64)
+        step = np.maximum(1.0, np.abs(s["step"]))
+        chain = s["filterTrack"] >= 0
+        filtered = (s["filters"]["type"] != 0).any(axis=1)
+        moving = (s["activeEnvelope"][:, 0] != 0) if len(s) else np.zeros(0, bool)
+        bank = frames * ch * 4 * step
+        src += float(np.sum((bank + frames * ch * 4 + np.where(filtered & moving, frames * 12, 0))[chain]))
+        rec += float(np.sum((frames * ch * 8 + np.where(moving, frames * 12, 0))[chain & filtered]))
+        mix += float(np.sum(np.where(chain, frames * ch * 4, bank))) + p.frames * 8
+    return {"source": src, "recurrence": rec, "mix": mix}
+
+
+def measured_peaks():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        peaks = json.loads(path.read_text())
+        return float(peaks["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_unit():
+    """DRAM bytes per voice-frame per kernel from the committed ncu summary."""
+    path = ROOT / "profiles" / "dram_traffic.txt"
+    table = {}
+    if path.exists():
+        for line in path.read_text().splitlines():
+            parts = line.split()
+            if len(parts) >= 2 and not line.startswith("#"):
+                try:
+                    table[parts[0]] = float(parts[1])
+                except ValueError:
+                    pass
+    return table
+
+
+def cpu_baseline(plans, bank, sample_jobs):
+    """The reference's render.cu built for the host (oracle/_ref), all cores, on the
+    first `sample_jobs` jobs; the oracle restatement when that build is absent."""
+    from oracle import oracle
+    sample = plans[:sample_jobs]
+    threads = os.cpu_count() or 1
+    try:
+        from oracle import reference
+        if not reference.available():
+            raise RuntimeError
+        synth, kind = reference.synthesize, "reference"
+    except Exception:
+        synth, kind = oracle.synthesize, "port"
+    start = time.perf_counter()
+    mix = synth(sample, bank, True, threads)
+    _, results = oracle.finish(mix, sample)
+    seconds = time.perf_counter() - start
+    audio = float(results["frames"].sum()) / RATE
+    return {"value": audio / seconds, "unit": "audio-s/s", "cores": threads, "kind": kind,
+            "sample": f"first {len(sample)} of {len(plans)} jobs ({audio:.1f} output audio-s), natural tail"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return
+    jobs = workload(args, 0)
+    plans, bank = plan_jobs(jobs)
+    sample = plans[:args.cpu_sample_jobs]
+    try:
+        from oracle import oracle, reference
+        if not reference.available():
+            reference.build()
+        kind = "reference" if reference.available() else "port"
+        synth = reference.synthesize if kind == "reference" else oracle.synthesize
+    except Exception as error:  # no host build of the reference and no restatement
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU path unavailable: {error}"}))
+        return
+    threads = os.cpu_count() or 1
+    times, audio = [], 0.0
+    for i in range(args.warmup + args.steps):
+        start = time.perf_counter()
+        mix = synth(sample, bank, True, threads)
+        _, results = oracle.finish(mix, sample)
+        elapsed = time.perf_counter() - start
+        audio = float(results["frames"].sum()) / RATE
+        if i >= args.warmup:
+            times.append(elapsed)
+    mean = sum(times) / len(times)
+    value = audio / mean
+    out = {"metric": METRIC, "value": value, "unit": "audio-s/s", "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SFZ/WAV/MIDI)", "impl": "reference",
+           "config": {"workload": WORKLOAD, "sample": f"first {len(sample)} jobs", "tail": "natural"},
+           "cpu_baseline": {"value": value, "unit": "audio-s/s", "cores": threads, "kind": kind,
+                            "sample": f"first {len(sample)} of {len(plans)} jobs per step"},
+           "e2e": {"value": value, "unit": "audio-s/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def run_b200(args):
+    import torch
+    rank, world, local = dist_info()
+    distributed = world > 1
+    if distributed:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    from claysampler_b200.renderer import Renderer
+
+    jobs = workload(args, rank)
+    plans, bank = plan_jobs(jobs)
+    renderer = Renderer(device=local, natural=True, batch_jobs=len(plans))
+    renderer.upload_samples(bank)
+    prepared = renderer.prepare(plans)
+    prepared.set_profile(True)
+    stream = torch.cuda.Stream()          # a real stream: handle 0 would mean the renderer's own
+
+    def barrier():
+        if distributed:
+            torch.distributed.barrier()
+
+    for _ in range(args.warmup):
+        prepared.run(stream.cuda_stream)
+    torch.cuda.synchronize()
+    _, results = prepared.collect()
+    audio = float(results["frames"].sum()) / RATE
+    statuses = np.bincount(results["status"], minlength=12).tolist()
+
+    stage_totals = {}
+    with ClockSampler(local) as clocks:
+        barrier()
+        torch.cuda.synchronize()
+        step_ms = []
+        for _ in range(args.steps):
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            prepared.run(stream.cuda_stream)
+            end.record(stream)
+            end.synchronize()
+            step_ms.append(start.elapsed_time(end))
+            for name, ms in prepared.stage_ms().items():
+                stage_totals[name] = stage_totals.get(name, 0.0) + ms
+        barrier()
+        torch.cuda.synchronize()
+    ms = sum(step_ms) / len(step_ms)
+    launches = prepared.launches * args.steps
+
+    # End to end through the public API: plans in host memory, PCM back to host.
+    e2e_renderer = Renderer(device=local, natural=True, batch_jobs=len(plans))
+    e2e_renderer.upload_samples(bank)
+    h2d = sum(p.spans.nbytes + p.points.nbytes + p.modulation.nbytes + p.track_offsets.nbytes for p in plans)
+    box = {}
+
+    def publish(batch, first):
+        box["pcm"] = batch.pcm.nbytes + batch.results.nbytes
+        box["audio"] = float(batch.results["frames"].sum()) / RATE
+
+    e2e_times = []
+    for i in range(args.warmup + args.steps):
+        barrier()
+        torch.cuda.synchronize()
+        start = time.perf_counter()
+        e2e_renderer.render_window(plans, publish)
+        elapsed = time.perf_counter() - start
+        if i >= args.warmup:
+            e2e_times.append(elapsed)
+    e2e_s = sum(e2e_times) / len(e2e_times)
+
+    totals = torch.tensor([audio, ms, e2e_s, box.get("audio", 0.0)], dtype=torch.float64, device="cuda")
+    if distributed:
+        gathered = [torch.zeros_like(totals) for _ in range(world)]
+        torch.distributed.all_gather(gathered, totals)
+        rows = torch.stack(gathered).cpu().numpy()
+        total_audio, max_ms, max_e2e, total_e2e_audio = rows[:, 0].sum(), rows[:, 1].max(), rows[:, 2].max(), rows[:, 3].sum()
+    else:
+        total_audio, max_ms, max_e2e, total_e2e_audio = audio, ms, e2e_s, box.get("audio", 0.0)
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        algorithmic = algorithmic_bytes(plans)
+        stage_ms = {k: v / args.steps for k, v in stage_totals.items()}
+        candidates = {k: stage_ms.get(k, 0.0) for k in ("source", "recurrence", "mix")}
+        dominant = max(candidates, key=candidates.get)
+        achieved = algorithmic[dominant] / (stage_ms[dominant] * 1e-3) / 1e9
+        per_unit = traffic_per_unit()
+        voice_frames = sum(p.voice_frames() for p in plans)
+        traffic = per_unit[dominant] * voice_frames if dominant in per_unit else None
+        out = {"metric": METRIC, "value": total_audio / (max_ms * 1e-3), "unit": "audio-s/s", "n_gpus": world,
+               "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SFZ/WAV/MIDI)",
+               "config": {"workload": WORKLOAD, "jobs_per_gpu": len(plans), "seed": args.seed,
+                          "output_audio_s_per_gpu": audio, "voice_frames_per_gpu": voice_frames,
+                          "tail": "natural", "taps": 48, "l2": "inputs larger than L2 (no flush)",
+                          "parallelism": f"jobs sharded by rank, {world} rank(s)", "statuses": statuses},
+               "stage_ms": stage_ms,
+               "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
+                            "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                            "algorithmic_bytes": algorithmic[dominant], "traffic": traffic},
+               "e2e": {"value": total_e2e_audio / max_e2e, "unit": "audio-s/s", "h2d_bytes_per_step": int(h2d),
+                       "d2h_bytes_per_step": int(box.get("pcm", 0)), "ms_per_step": max_e2e * 1e3},
+               "gpu_launches": launches, "clocks": clocks.summary()}
+        if world == 1:
+            try:
+                out["cpu_baseline"] = cpu_baseline(plans, bank, args.cpu_sample_jobs)
+            except Exception as error:
+                out["cpu_baseline"] = {"value": None, "unavailable": str(error)}
+        print(json.dumps(out))
+    prepared.close()
+    renderer.close()
+    e2e_renderer.close()
+    if distributed:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

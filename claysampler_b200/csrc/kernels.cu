@@ -1147,30 +1147,36 @@ void launchPitch(const BatchView& b, const SegmentView& s, cudaStream_t stream)
     pitchKernel<<<(s.pitchCount + 63) / 64, 64, 0, stream>>>(b, s);
 }
 
-int launchChains(const BatchView& b, const SegmentView& s, cudaStream_t stream)
+int launchSources(const BatchView& b, const SegmentView& s, cudaStream_t stream)
 {
-    int launches = 0;
-    if (s.sourceTileCount) {
-        sourceKernel<<<s.sourceTileCount, kSourceTile, 0, stream>>>(b, s);
-        ++launches;
+    if (!s.sourceTileCount)
+        return 0;
+    sourceKernel<<<s.sourceTileCount, kSourceTile, 0, stream>>>(b, s);
+    return 1;
+}
+
+int launchRecurrences(const BatchView& b, const SegmentView& s, cudaStream_t stream)
+{
+    if (!s.simpleCount)
+        return 0;
+    constexpr int chainsPerCta = kRecWarps * kRecChains;
+    constexpr int bytes = chainsPerCta * kRecChainBytes;
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(recurrenceKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        configured = true;
     }
-    if (s.simpleCount) {
-        constexpr int chainsPerCta = kRecWarps * kRecChains;
-        constexpr int bytes = chainsPerCta * kRecChainBytes;
-        static bool configured = false;
-        if (!configured) {
-            cudaFuncSetAttribute(recurrenceKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-            configured = true;
-        }
-        recurrenceKernel<<<(s.simpleCount + chainsPerCta - 1) / chainsPerCta, kRecThreads, bytes, stream>>>(
-            b, s, b.error);
-        ++launches;
-    }
-    if (s.chainCount) {
-        chainKernel<<<(s.chainCount + kChainWarps - 1) / kChainWarps, kChainWarps * 32, 0, stream>>>(b, s);
-        ++launches;
-    }
-    return launches;
+    recurrenceKernel<<<(s.simpleCount + chainsPerCta - 1) / chainsPerCta, kRecThreads, bytes, stream>>>(
+        b, s, b.error);
+    return 1;
+}
+
+int launchGeneralChains(const BatchView& b, const SegmentView& s, cudaStream_t stream)
+{
+    if (!s.chainCount)
+        return 0;
+    chainKernel<<<(s.chainCount + kChainWarps - 1) / kChainWarps, kChainWarps * 32, 0, stream>>>(b, s);
+    return 1;
 }
 
 void launchMix(const BatchView& b, const SegmentView& s, bool natural, StereoStats* stats, cudaStream_t stream)

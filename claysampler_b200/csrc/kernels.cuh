@@ -99,7 +99,9 @@ struct FinishView {
 void buildSincTable(float* phaseMajor);   // host: 2049 x 48 floats
 
 void launchPitch(const BatchView& b, const SegmentView& s, cudaStream_t stream);
-int launchChains(const BatchView& b, const SegmentView& s, cudaStream_t stream);
+int launchSources(const BatchView& b, const SegmentView& s, cudaStream_t stream);
+int launchRecurrences(const BatchView& b, const SegmentView& s, cudaStream_t stream);
+int launchGeneralChains(const BatchView& b, const SegmentView& s, cudaStream_t stream);
 void launchMix(const BatchView& b, const SegmentView& s, bool natural, StereoStats* stats, cudaStream_t stream);
 int launchFinish(const BatchView& b, const FinishView& f, bool natural, bool quality, const TailConfig& tail,
                  cudaStream_t stream);

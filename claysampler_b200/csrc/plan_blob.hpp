@@ -11,6 +11,7 @@
 
 #include "../../include/claysampler_b200.h"
 
+#include <cstddef>
 #include <cstring>
 #include <stdexcept>
 #include <vector>
@@ -46,7 +47,15 @@ inline std::vector<unsigned char> writePlanBlob(const cs_plan& plan)
     put(fields, sizeof fields);
     const uint64_t tail[2] = {plan.volume_group, uint64_t(points)};
     put(tail, sizeof tail);
-    put(plan.spans, size_t(plan.span_count) * sizeof(cs_voice_span));
+    // Spans are written with their one padding gap (after nextFilteredSpan) zeroed,
+    // so equal plans have equal images.
+    constexpr size_t gap = offsetof(cs_voice_span, nextFilteredSpan) + sizeof(int32_t);
+    static_assert(offsetof(cs_voice_span, filteredOffset) - gap == 4, "cs_voice_span padding");
+    for (int s = 0; s < plan.span_count; ++s) {
+        unsigned char* at = p;
+        put(&plan.spans[s], sizeof(cs_voice_span));
+        std::memset(at + gap, 0, 4);
+    }
     if (plan.track_count) {
         put(plan.track_offsets, size_t(plan.track_count + 1) * sizeof(int64_t));
     } else {

@@ -11,6 +11,7 @@
 #include "plan_blob.hpp"
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -55,7 +56,10 @@ struct Layout {
 // control and modulation offsets, and voice chains linked by nextFilteredSpan.
 struct HostBatch {
     std::vector<cs_voice_span> voices;
-    std::vector<cs_control_point> points;
+    // Control points stay in the callers' plans; each plan's points are copied once,
+    // straight into the pinned upload buffer.
+    std::vector<std::pair<const cs_control_point*, size_t>> pointSources;
+    size_t pointCount = 0;
     std::vector<cs_voice_modulation> modulation;
     std::vector<JobInfo> jobs;
     std::vector<MixTile> tiles;
@@ -80,11 +84,14 @@ struct HostBatch {
         job.windowFirst = windows;
         job.tileFirst = int(tiles.size());
         std::vector<int> pointOffsets(size_t(plan.track_count) + 1);
-        pointOffsets[0] = int(points.size());
-        for (int i = 0; i < plan.track_count; ++i) {
-            points.insert(points.end(), plan.points + plan.track_offsets[i], plan.points + plan.track_offsets[i + 1]);
-            pointOffsets[size_t(i) + 1] = int(points.size());
-        }
+        const int64_t planPoints = plan.track_offsets[plan.track_count] - plan.track_offsets[0];
+        if (pointCount + size_t(planPoints) > size_t(INT32_MAX))
+            throw std::runtime_error("too many control points in one batch");
+        for (int i = 0; i <= plan.track_count; ++i)
+            pointOffsets[size_t(i)] = int(pointCount + size_t(plan.track_offsets[i] - plan.track_offsets[0]));
+        if (planPoints)
+            pointSources.emplace_back(plan.points + plan.track_offsets[0], size_t(planPoints));
+        pointCount += size_t(planPoints);
         for (int i = 0; i < 4; ++i)
             job.tracks[i] = pointOffsets[size_t(i)];
         const int modulationBase = int(modulation.size());
@@ -374,6 +381,7 @@ SegmentTables planSegments(const HostBatch& batch, size_t budget)
 
 struct cs_prepared {
     cs_renderer* owner = nullptr;
+    bool sharedArena = false;
     cs::HostBatch batch;
     cs::SegmentTables tables;
     void* arena = nullptr;
@@ -388,6 +396,10 @@ struct cs_prepared {
     cudaEvent_t begin = nullptr, end = nullptr;
     std::vector<cs_tail_result> results;
     bool ran = false;
+    // Optional per-stage timing: an event after every stage of the last run.
+    bool profile = false;
+    std::vector<cudaEvent_t> marks;
+    std::vector<int> markStage;
 };
 
 struct cs_renderer {
@@ -407,6 +419,29 @@ struct cs_renderer {
     size_t live = 0;                    // bytes of prepared batches alive
     void* hostPcm = nullptr;
     size_t hostPcmCapacity = 0;
+    void* staging = nullptr;            // pinned upload buffer for batch metadata
+    size_t stagingCapacity = 0;
+    void* arena = nullptr;              // device arena reused by render_window batches
+    size_t arenaCapacity = 0;
+
+    // Page-locked host memory that grows on demand (the copy engines read and write
+    // it directly).
+    static void* pinned(void*& buffer, size_t& capacity, size_t bytes)
+    {
+        if (bytes <= capacity && buffer)
+            return buffer;
+        if (buffer)
+            cudaFreeHost(buffer);
+        buffer = nullptr;
+        capacity = 0;
+        const size_t want = std::max<size_t>(bytes + bytes / 4, size_t(1) << 20);
+        if (cudaMallocHost(&buffer, want) != cudaSuccess) {
+            cudaGetLastError();
+            throw std::runtime_error("cannot allocate pinned host memory");
+        }
+        capacity = want;
+        return buffer;
+    }
 
     void record(size_t extra = 0)
     {
@@ -427,7 +462,9 @@ size_t defaultScratchBudget()
     return std::max<size_t>(size_t(1) << 20, std::min(freeBytes / 2, total / 4));
 }
 
-cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count)
+// `shared`: carve the batch from the renderer's reusable arena (render_window
+// batches, one alive at a time) instead of a dedicated allocation.
+cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool shared = false)
 {
     check(cudaSetDevice(r.device), "CUDA device");
     auto p = std::make_unique<cs_prepared>();
@@ -445,7 +482,7 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count)
     Layout layout;
     const auto section = [&](size_t bytes) { return layout.add(std::max<size_t>(bytes, 1)); };
     const size_t oVoices = section(batch.voices.size() * sizeof(cs_voice_span));
-    const size_t oPoints = section(batch.points.size() * sizeof(cs_control_point));
+    const size_t oPoints = section(batch.pointCount * sizeof(cs_control_point));
     const size_t oMods = section(batch.modulation.size() * sizeof(cs_voice_modulation));
     const size_t oJobs = section(jobs * sizeof(JobInfo));
     const size_t oTiles = section(batch.tiles.size() * sizeof(MixTile));
@@ -475,22 +512,47 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count)
     const size_t oError = section(sizeof(int));
     p->arenaBytes = layout.bytes;
 
-    cudaError_t status = cudaMalloc(&p->arena, p->arenaBytes);
-    if (status != cudaSuccess) {
-        cudaGetLastError();
-        p->arena = nullptr;
-        throw CudaError(status, "CUDA batch arena allocation");
+    if (shared) {
+        if (p->arenaBytes > r.arenaCapacity) {
+            cudaFree(r.arena);
+            r.live -= r.arenaCapacity;
+            r.arena = nullptr;
+            r.arenaCapacity = 0;
+            cudaError_t status = cudaMalloc(&r.arena, p->arenaBytes);
+            if (status != cudaSuccess) {
+                cudaGetLastError();
+                r.arena = nullptr;
+                throw CudaError(status, "CUDA batch arena allocation");
+            }
+            r.arenaCapacity = p->arenaBytes;
+            r.live += r.arenaCapacity;
+        }
+        p->arena = r.arena;
+        p->sharedArena = true;
+    } else {
+        cudaError_t status = cudaMalloc(&p->arena, p->arenaBytes);
+        if (status != cudaSuccess) {
+            cudaGetLastError();
+            p->arena = nullptr;
+            throw CudaError(status, "CUDA batch arena allocation");
+        }
+        r.live += p->arenaBytes;
     }
-    r.live += p->arenaBytes;
     r.record();
     auto* base = static_cast<unsigned char*>(p->arena);
-    std::vector<unsigned char> staging(uploadEnd, 0);
+    auto* staging = static_cast<unsigned char*>(cs_renderer::pinned(r.staging, r.stagingCapacity, uploadEnd));
     const auto stage = [&](size_t offset, const auto& items) {
         if (!items.empty())
-            std::memcpy(staging.data() + offset, items.data(), items.size() * sizeof(items.front()));
+            std::memcpy(staging + offset, items.data(), items.size() * sizeof(items.front()));
     };
     stage(oVoices, batch.voices);
-    stage(oPoints, batch.points);
+    {
+        unsigned char* at = staging + oPoints;
+        for (const auto& [first, count] : batch.pointSources) {
+            std::memcpy(at, first, count * sizeof(cs_control_point));
+            at += count * sizeof(cs_control_point);
+        }
+    }
     stage(oMods, batch.modulation);
     stage(oJobs, batch.jobs);
     stage(oTiles, batch.tiles);
@@ -505,7 +567,7 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count)
     stage(oSimple, t.simple);
     stage(oPitch, t.pitch);
     stage(oBlocks, t.blocks);
-    check(cudaMemcpyAsync(base, staging.data(), uploadEnd, cudaMemcpyHostToDevice, r.stream), "CUDA batch upload");
+    check(cudaMemcpyAsync(base, staging, uploadEnd, cudaMemcpyHostToDevice, r.stream), "CUDA batch upload");
     check(cudaStreamSynchronize(r.stream), "CUDA batch upload");
 
     BatchView& v = p->view;
@@ -561,6 +623,9 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count)
     return p.release();
 }
 
+const char* const kStageNames[] = {"pitch", "source", "recurrence", "general", "mix", "finish"};
+constexpr int kStages = 6;
+
 void run(cs_renderer& r, cs_prepared& p, cudaStream_t stream)
 {
     check(cudaSetDevice(r.device), "CUDA device");
@@ -569,10 +634,24 @@ void run(cs_renderer& r, cs_prepared& p, cudaStream_t stream)
     p.view.bank = r.bank;
     p.view.sinc = r.sinc;
     int launches = 0;
+    size_t mark = 0;
+    p.markStage.clear();
+    const auto stage = [&](int id) {
+        if (!p.profile)
+            return;
+        if (mark == p.marks.size()) {
+            cudaEvent_t e;
+            check(cudaEventCreate(&e), "CUDA timing event");
+            p.marks.push_back(e);
+        }
+        check(cudaEventRecord(p.marks[mark++], stream), "CUDA timing record");
+        p.markStage.push_back(id);
+    };
     check(cudaEventRecord(p.begin, stream), "CUDA timing record");
     check(cudaMemsetAsync(p.view.states, 0, std::max<size_t>(p.stateBytes, 1), stream), "CUDA state reset");
     check(cudaMemsetAsync(p.finish.results, 0, std::max<size_t>(p.resultBytes, 1), stream), "CUDA result reset");
     check(cudaMemsetAsync(p.view.error, 0, sizeof(int), stream), "CUDA error flag reset");
+    stage(-1);
     for (size_t i = 0; i < p.segments.size(); ++i) {
         BatchView view = p.view;
         const SegmentPlan& plan = p.tables.segments[i];
@@ -580,12 +659,21 @@ void run(cs_renderer& r, cs_prepared& p, cudaStream_t stream)
                                                align256(plan.scratchFloats * sizeof(float)));
         const SegmentView& s = p.segments[i];
         launchPitch(view, s, stream);
-        launches += launchChains(view, s, stream);
+        launches += s.pitchCount > 0;
+        stage(0);
+        launches += launchSources(view, s, stream);
+        stage(1);
+        launches += launchRecurrences(view, s, stream);
+        stage(2);
+        launches += launchGeneralChains(view, s, stream);
+        stage(3);
         launchMix(view, s, r.natural, p.stereo, stream);
-        launches += (s.pitchCount > 0) + (s.blockCount > 0);
+        launches += s.blockCount > 0;
+        stage(4);
     }
     check(cudaGetLastError(), "CUDA synthesis launch");
     launches += launchFinish(p.view, p.finish, r.natural, r.audio.enabled != 0, r.tail, stream);
+    stage(5);
     check(cudaGetLastError(), "CUDA finishing launch");
     check(cudaEventRecord(p.end, stream), "CUDA timing record");
     p.launches = launches;
@@ -693,7 +781,9 @@ void cs_renderer_destroy(cs_renderer* r)
     if (r->stream) cudaStreamSynchronize(r->stream);
     cudaFree(r->sinc);
     cudaFree(r->bank);
+    cudaFree(r->arena);
     if (r->hostPcm) cudaFreeHost(r->hostPcm);
+    if (r->staging) cudaFreeHost(r->staging);
     if (r->stream) cudaStreamDestroy(r->stream);
     delete r;
 }
@@ -784,6 +874,38 @@ int cs_copy_mix(cs_renderer* r, cs_prepared* p, void* host, size_t bytes)
 }
 
 size_t cs_prepared_frames(const cs_prepared* p) { return p ? p->batch.frames : 0; }
+
+int cs_prepared_set_profile(cs_prepared* p, int enable)
+{
+    return cs::guarded([&] {
+        if (!p)
+            throw std::runtime_error("null batch");
+        p->profile = enable != 0;
+    });
+}
+
+int cs_prepared_stage_ms(cs_prepared* p, float* ms, int capacity)
+{
+    int stages = 0;
+    const int status = cs::guarded([&] {
+        if (!p || !p->ran || !p->profile)
+            throw std::runtime_error("batch has no profiled run");
+        cs::check(cudaEventSynchronize(p->end), "CUDA render completion");
+        for (int i = 0; i < capacity; ++i)
+            ms[i] = 0;
+        for (size_t k = 1; k < p->markStage.size(); ++k) {
+            float elapsed = 0;
+            cs::check(cudaEventElapsedTime(&elapsed, p->marks[k - 1], p->marks[k]), "CUDA stage timing");
+            const int id = p->markStage[k];
+            if (id >= 0 && id < capacity)
+                ms[id] += elapsed;
+        }
+        stages = cs::kStages;
+    });
+    return status ? -1 : stages;
+}
+
+const char* cs_stage_name(int stage) { return stage >= 0 && stage < cs::kStages ? cs::kStageNames[stage] : ""; }
 int cs_prepared_launches(const cs_prepared* p) { return p ? p->launches : 0; }
 
 void cs_prepared_destroy(cs_prepared* p)
@@ -791,9 +913,11 @@ void cs_prepared_destroy(cs_prepared* p)
     if (!p)
         return;
     if (p->end) cudaEventSynchronize(p->end);
+    for (cudaEvent_t e : p->marks)
+        cudaEventDestroy(e);
     if (p->begin) cudaEventDestroy(p->begin);
     if (p->end) cudaEventDestroy(p->end);
-    if (p->arena) {
+    if (p->arena && !p->sharedArena) {
         cudaFree(p->arena);
         if (p->owner)
             p->owner->live -= p->arenaBytes;
@@ -810,7 +934,6 @@ int cs_render_window(cs_renderer* r, const cs_plan* plans, size_t count, cs_publ
         std::vector<cs_plan> queue(plans, plans + count);
         cs::checkPlans(plans, count);
         size_t first = 0;
-        std::vector<int16_t> pcm;
         for (;;) {
             if (first == queue.size()) {
                 const cs_plan* more = nullptr;
@@ -824,7 +947,7 @@ int cs_render_window(cs_renderer* r, const cs_plan* plans, size_t count, cs_publ
             cs_prepared* prepared = nullptr;
             for (;;) {
                 try {
-                    prepared = cs::prepare(*r, queue.data() + first, jobs);
+                    prepared = cs::prepare(*r, queue.data() + first, jobs, true);
                     break;
                 } catch (const cs::CudaError& e) {
                     if (e.code != cudaErrorMemoryAllocation)
@@ -848,15 +971,16 @@ int cs_render_window(cs_renderer* r, const cs_plan* plans, size_t count, cs_publ
             std::unique_ptr<cs_prepared, void (*)(cs_prepared*)> guard(prepared, cs_prepared_destroy);
             cs::run(*r, *prepared, nullptr);
             const size_t samples = cs::collectResults(*r, *prepared);
-            pcm.resize(samples);
+            auto* pcm = static_cast<int16_t*>(
+                cs_renderer::pinned(r->hostPcm, r->hostPcmCapacity, std::max<size_t>(samples, 1) * sizeof(int16_t)));
             if (samples)
-                cs::check(cudaMemcpy(pcm.data(), prepared->finish.packed, samples * sizeof(int16_t),
+                cs::check(cudaMemcpy(pcm, prepared->finish.packed, samples * sizeof(int16_t),
                                      cudaMemcpyDeviceToHost), "CUDA PCM download");
             r->downloaded += samples * sizeof(int16_t);
             float ms = 0;
             cs::check(cudaEventElapsedTime(&ms, prepared->begin, prepared->end), "CUDA kernel timing");
             cs_batch batch{};
-            batch.pcm = pcm.data();
+            batch.pcm = pcm;
             batch.pcm_samples = samples;
             batch.results = prepared->results.data();
             batch.result_count = prepared->results.size();

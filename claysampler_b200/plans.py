@@ -93,9 +93,11 @@ class Plan:
         offset = _HEADER.size
 
         def take(dtype, count):
+            # Copy raw bytes (numpy's copy of a padded record dtype drops the padding).
             nonlocal offset
-            array = np.frombuffer(blob, dtype=dtype, count=count, offset=offset).copy()
-            offset += array.nbytes
+            nbytes = np.dtype(dtype).itemsize * count
+            array = np.frombuffer(bytearray(blob[offset:offset + nbytes]), dtype=dtype, count=count)
+            offset += nbytes
             return array
         plan = cls(take(VOICE_SPAN, spans), None, None, None, None, filter_tracks, frames, music_end, limit,
                    fade_frames, tail_clipped, body_frames, group)

@@ -53,6 +53,9 @@ def library() -> ctypes.CDLL:
         lib.cs_prepared_segments.restype = sz
         lib.cs_prepared_destroy.argtypes = [vp]
         lib.cs_renderer_set_scratch_limit.argtypes = [vp, sz]
+        lib.cs_prepared_set_profile.argtypes = [vp, i32]
+        lib.cs_prepared_stage_ms.argtypes = [vp, vp, i32]
+        lib.cs_stage_name.restype = c.c_char_p
         _lib = lib
     return _lib
 
@@ -106,6 +109,17 @@ class Prepared:
     @property
     def segments(self) -> int:
         return library().cs_prepared_segments(self.handle)
+
+    def set_profile(self, enable: bool = True) -> None:
+        _check(library().cs_prepared_set_profile(self.handle, int(enable)))
+
+    def stage_ms(self) -> dict[str, float]:
+        """Device time of each stage of the last profiled run (CUDA events)."""
+        out = (ctypes.c_float * 8)()
+        count = library().cs_prepared_stage_ms(self.handle, out, 8)
+        if count < 0:
+            _check(1)
+        return {library().cs_stage_name(i).decode(): float(out[i]) for i in range(count)}
 
     def run(self, stream: int | None = None) -> None:
         _check(library().cs_run(self.renderer.handle, self.handle, stream))

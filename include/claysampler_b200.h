@@ -223,6 +223,14 @@ size_t cs_prepared_frames(const cs_prepared* batch);
 /* Kernel launches the last cs_run enqueued. */
 int cs_prepared_launches(const cs_prepared* batch);
 void cs_prepared_destroy(cs_prepared* batch);
+/* Per-stage device timing of the next cs_run calls (events between stages). */
+int cs_prepared_set_profile(cs_prepared* batch, int enable);
+/* Fills ms[stage] (stages: 0 pitch, 1 source, 2 recurrence, 3 general chains,
+ * 4 mix + block scan, 5 finishing) for the last profiled run; returns the stage
+ * count or -1. */
+int cs_prepared_stage_ms(cs_prepared* batch, float* ms, int capacity);
+const char* cs_stage_name(int stage);
+
 /* Number of synthesis segments the batch was cut into. */
 size_t cs_prepared_segments(const cs_prepared* batch);
 
