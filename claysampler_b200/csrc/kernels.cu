@@ -889,6 +889,36 @@ __global__ void __launch_bounds__(kMixThreads) mixKernel(BatchView b, SegmentVie
     }
 }
 
+// Power and peak of each 1024-frame block of an existing float mix (the block scan
+// that mixKernel fuses into synthesis, for a mix produced elsewhere).
+__global__ void __launch_bounds__(kMixThreads) scanKernel(BatchView b, StereoStats* stats, int blocks)
+{
+    __shared__ double reduceD[32];
+    __shared__ float reduceF[32];
+    const int block = int(blockIdx.x);
+    if (block >= blocks)
+        return;
+    const JobInfo job = b.jobs[b.blockJob[block]];
+    const int first = (block - job.blockFirst) * kBlockFrames;
+    const int end = min(first + kBlockFrames, job.frames);
+    const float2* mix = static_cast<const float2*>(b.mix) + job.offset;
+    double power = 0;
+    float peak = 0;
+    for (int frame = first + int(threadIdx.x); frame < end; frame += blockDim.x) {
+        const float2 v = mix[frame];
+        if (!isfinite(v.x) || !isfinite(v.y)) {
+            peak = __int_as_float(0x7f800000);
+        } else {
+            peak = fmaxf(peak, fmaxf(fabsf(v.x), fabsf(v.y)));
+            power += double(__fmul_rn(v.x, v.x)) + double(__fmul_rn(v.y, v.y));
+        }
+    }
+    power = blockReduce(power, 0.0, SumOp{}, reduceD);
+    peak = blockReduce(peak, 0.f, MaxOp{}, reduceF);
+    if (threadIdx.x == 0)
+        stats[block] = {power, peak};
+}
+
 // ---- finishing (src/cuda/tail.cu) ------------------------------------------------------
 
 // Natural endpoint, peak repair and scale, one warp per job (tail.cu:83-139).
@@ -1139,6 +1169,12 @@ __global__ void finalizeKernel(BatchView b, FinishView f, const short* input, in
 }
 
 // ---- launchers --------------------------------------------------------------------------
+
+void launchScan(const BatchView& b, StereoStats* stats, int blocks, cudaStream_t stream)
+{
+    if (blocks)
+        scanKernel<<<blocks, kMixThreads, 0, stream>>>(b, stats, blocks);
+}
 
 void launchPitch(const BatchView& b, const SegmentView& s, cudaStream_t stream)
 {

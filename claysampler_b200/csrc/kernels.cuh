@@ -98,6 +98,7 @@ struct FinishView {
 
 void buildSincTable(float* phaseMajor);   // host: 2049 x 48 floats
 
+void launchScan(const BatchView& b, StereoStats* stats, int blocks, cudaStream_t stream);
 void launchPitch(const BatchView& b, const SegmentView& s, cudaStream_t stream);
 int launchSources(const BatchView& b, const SegmentView& s, cudaStream_t stream);
 int launchRecurrences(const BatchView& b, const SegmentView& s, cudaStream_t stream);

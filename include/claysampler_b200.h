@@ -240,6 +240,36 @@ size_t cs_prepared_segments(const cs_prepared* batch);
  * (docs/validation.md:145). */
 int cs_renderer_set_scratch_limit(cs_renderer* renderer, size_t bytes);
 
+/* ---- natural-tail finishing without device allocation --------------------------
+ * No counterpart in the reference (its finishing always runs inside the renderer
+ * on renderer-owned scratch).  For callers that cannot allocate device memory
+ * while they render: a real-time audio host calling in from its audio callback,
+ * where cudaMalloc can block or synchronise the device past the callback's
+ * deadline, or an application embedding the renderer that owns the device-memory
+ * budget itself.  The caller passes the float mix (float2 per frame, jobs
+ * concatenated in order) and the outputs, all in device memory; the stage's
+ * intermediates live in a fixed file-scope device array of about 17 MiB that every
+ * GPU loading the library holds until exit.  Limits per call:
+ * CS_STATIC_FINISH_MAX_FRAMES frames and CS_STATIC_FINISH_MAX_JOBS jobs (larger
+ * calls fail with a message from cs_finish_natural_static_error); window >= 400.
+ * The first call on each device looks up the array's device address with that
+ * device current, so make it before any stream capture.  All calls share the
+ * array: calls whose work overlaps on the GPU race and must be serialised.
+ * `packed` receives up to the sum of frames int16 samples and `results` one
+ * cs_tail_result per job, exactly as the renderer's natural finishing writes
+ * them.  Enqueued on `stream` (a cudaStream_t; NULL = the legacy default stream);
+ * returns 0 once enqueued. */
+#define CS_STATIC_FINISH_MAX_FRAMES (1u << 23)
+#define CS_STATIC_FINISH_MAX_JOBS 256
+
+typedef struct cs_finish_job {
+    int32_t frames, music_end, limit, fade_frames;
+} cs_finish_job;
+
+int cs_finish_natural_static(const float* mix, const cs_finish_job* jobs, int count, int rate, int window,
+                             int16_t* packed, cs_tail_result* results, void* stream);
+const char* cs_finish_natural_static_error(void);
+
 #ifdef __cplusplus
 }
 #endif
