@@ -99,3 +99,22 @@ def test_segmented_synthesis_is_byte_identical(batch_mini, ref_session):
     assert np.array_equal(mix.view(np.uint32), mix2.view(np.uint32))
     assert np.array_equal(pcm, pcm2)
     assert results.tobytes() == results2.tobytes()
+
+
+@pytest.mark.parametrize("fixture", ["plain_small", "batch_mini"])
+def test_host_planned_batch_matches_oracle(request, fixture):
+    """Self-contained on any GPU box: this package's planner feeds both the GPU
+    path and the oracle's restatement of the reference render (no reference build
+    needed)."""
+    from claysampler_b200.host import Host
+    from oracle import oracle
+    jobs = request.getfixturevalue(fixture)
+    host = Host()
+    plans = [host.plan(j.sfz, j.midi) for j in jobs]
+    bank = host.bank()
+    mix, pcm, results, _ = render(plans, bank, True)
+    expected_mix = oracle.synthesize(plans, bank, True)
+    assert float(np.max(np.abs(mix - expected_mix))) <= BUS_TOLERANCE
+    expected_pcm, expected = oracle.finish(expected_mix, plans, True)
+    compare_results(results, expected)
+    compare_pcm(pcm, expected_pcm)

@@ -1,0 +1,63 @@
+"""The oracle's plain-C restatement of the render path, pinned against the
+reference's own code built for the host (oracle/_ref) and against the golden
+vectors the reference's tests assert."""
+import numpy as np
+import pytest
+
+from claysampler_b200 import workload
+
+
+def ref_or_skip():
+    from oracle import reference
+    if not (reference.available() or reference.build()):
+        pytest.skip("oracle/_ref (the reference built for the host) is not available")
+    return reference
+
+
+def test_sinc_table_matches_reference():
+    from oracle import oracle
+    reference = ref_or_skip()
+    mine = np.zeros(48 * 2049, np.float32)
+    oracle.lib().oracle_sinc_table(mine.ctypes.data)
+    assert np.array_equal(mine.view(np.uint32), reference.sinc_table().reshape(-1).view(np.uint32))
+
+
+@pytest.mark.parametrize("tail", ["natural", "orig"])
+@pytest.mark.parametrize("fixture", ["plain_small", "batch_mini"])
+def test_restated_render_matches_reference_bit_for_bit(request, ref_session, fixture, tail):
+    from oracle import oracle
+    reference = ref_or_skip()
+    jobs = request.getfixturevalue(fixture)
+    plans = [ref_session.plan(j.sfz, j.midi, tail=tail) for j in jobs]
+    bank = ref_session.bank()
+    natural = tail == "natural"
+    theirs = reference.synthesize(plans, bank, natural)
+    mine = oracle.synthesize(plans, bank, natural)
+    assert np.array_equal(mine.view(np.uint32 if natural else np.uint16), theirs.view(np.uint32 if natural else np.uint16))
+
+
+def test_restated_render_pitch_and_bends(tmp_path, ref_session):
+    """Variable pitch (LFO to pitch), bends, CC-driven cutoff: the reference's
+    check_segments.py voice and check_tail.py's processed preset."""
+    import struct
+    import wave
+    from oracle import oracle
+    reference = ref_or_skip()
+    rate = 44100
+    with wave.open(str(tmp_path / "sample.wav"), "wb") as stream:
+        stream.setparams((1, 2, rate, 0, "NONE", "not compressed"))
+        stream.writeframes(b"".join(struct.pack("<h", round(3000 * np.sin(i * .04))) for i in range(rate)))
+    sfz = tmp_path / "voice.sfz"
+    sfz.write_text("<region> sample=sample.wav key=60 loop_mode=loop_continuous loop_start=0 loop_end=44099 "
+                   "amp_veltrack=0 ampeg_release=1.7 cutoff=1800 resonance=3 cutoff_oncc1=3000 pitch_oncc1=37 "
+                   "lfo1_freq=3 lfo1_pitch=120\n", encoding="ascii")
+    data = bytes.fromhex("00 b0 40 7f 00 90 3c 64 87 40 b0 01 40 87 40 e0 00 50 87 40 80 3c 00 87 40 b0 40 00 00 ff 2f 00")
+    midi = tmp_path / "long.mid"
+    midi.write_bytes(b"MThd" + struct.pack(">IHHH", 6, 0, 1, 480) + b"MTrk" + struct.pack(">I", len(data)) + data)
+    plans = [ref_session.plan(sfz, midi, tail="orig")]
+    assert plans[0].spans["variablePitch"].any()
+    bank = ref_session.bank()
+    for natural in (True, False):
+        theirs = reference.synthesize(plans, bank, natural)
+        mine = oracle.synthesize(plans, bank, natural)
+        assert np.array_equal(mine.view(np.uint32 if natural else np.uint16), theirs.view(np.uint32 if natural else np.uint16))
