@@ -50,7 +50,7 @@ def parse():
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
     p.add_argument("--jobs", type=int, default=64)
     p.add_argument("--seed", type=int, default=2)
-    p.add_argument("--cpu-sample-jobs", type=int, default=8)
+    p.add_argument("--cpu-sample-jobs", type=int, default=32)
     p.add_argument("--workdir", type=Path, default=Path(tempfile.gettempdir()) / "claysampler_bench")
     return p.parse_args()
 
