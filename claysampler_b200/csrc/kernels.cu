@@ -1118,11 +1118,16 @@ __device__ __forceinline__ short fadeSample(short value, int index, int count)
     return short(__double2int_rn(value * gain));
 }
 
-// Fade, compaction and peak / audible range (tail.cu:240-297).
+// Fade, compaction and peak / audible range (tail.cu:240-297).  When the quality
+// gate or group volume is on, the same pass sums the mono power of the samples it
+// writes into the job's 250 ms body windows (measureBody, quality.cu:21-39): the
+// sums are integers, so the block partials and atomics give the reference's
+// totals in any order.
 template <int Channels>
 __global__ void finalizeKernel(BatchView b, FinishView f, const short* input, int quality)
 {
     __shared__ int reduceI[32];
+    __shared__ unsigned long long reduceU[32];
     const int block = int(blockIdx.x);
     const int jobIndex = b.blockJob[block];
     const JobInfo job = b.jobs[jobIndex];
@@ -1133,10 +1138,25 @@ __global__ void finalizeKernel(BatchView b, FinishView f, const short* input, in
     const int end = min(first + kBlockFrames, result.dataFrames);
     if (first >= end)
         return;
+    // Body windows this block touches: [windowA, windowB]; frames before `split`
+    // belong to windowA.
+    int bodyEnd = 0, windowA = 0, windowB = 0, split = 0, bodyFirst = 0;
+    if (f.bodyPower && result.status == CS_TAIL_OK) {
+        const AssessJob a = f.assess[jobIndex];
+        bodyEnd = min(a.bodyFrames, end);
+        bodyFirst = a.bodyFirst;
+        if (first < bodyEnd) {
+            windowA = f.body.windowOf(first);
+            windowB = f.body.windowOf(bodyEnd - 1);
+            split = f.body.start(windowA + 1);
+        }
+    }
+    const bool paired = windowB - windowA <= 1;
+    unsigned long long powerA = 0, powerB = 0;
     int peak = 0, audibleFirst = frames, audibleLast = -1, clipped = 0;
     const int fadeStart = frames - fade;
     for (int frame = first + int(threadIdx.x); frame < end; frame += blockDim.x) {
-        int framePeak = 0;
+        int framePeak = 0, mono = 0;
         #pragma unroll
         for (int c = 0; c < Channels; ++c) {
             short value = input[(job.offset + frame) * Channels + c];
@@ -1146,17 +1166,36 @@ __global__ void finalizeKernel(BatchView b, FinishView f, const short* input, in
             const int magnitude = abs(int(value));
             framePeak = max(framePeak, magnitude);
             clipped += magnitude >= 32767;
+            mono += Channels == 1 ? 2 * int(value) : int(value);
         }
         peak = max(peak, framePeak);
         if (framePeak > 3) {
             audibleFirst = min(audibleFirst, frame);
             audibleLast = frame;
         }
+        if (frame < bodyEnd) {
+            const unsigned long long power = (unsigned long long)((long long)mono * mono);
+            if (!paired)
+                atomicAdd(f.bodyPower + bodyFirst + f.body.windowOf(frame), power);
+            else if (frame < split)
+                powerA += power;
+            else
+                powerB += power;
+        }
     }
     peak = blockReduce(peak, 0, MaxOp{}, reduceI);
     audibleFirst = blockReduce(audibleFirst, frames, MinOp{}, reduceI);
     audibleLast = blockReduce(audibleLast, -1, MaxOp{}, reduceI);
     clipped = blockReduce(clipped, 0, SumOp{}, reduceI);
+    if (first < bodyEnd && paired) {          // uniform across the block
+        powerA = blockReduce(powerA, 0ull, SumOp{}, reduceU);
+        powerB = blockReduce(powerB, 0ull, SumOp{}, reduceU);
+        if (threadIdx.x == 0) {
+            atomicAdd(f.bodyPower + bodyFirst + windowA, powerA);
+            if (windowB != windowA)
+                atomicAdd(f.bodyPower + bodyFirst + windowB, powerB);
+        }
+    }
     if (threadIdx.x == 0) {
         if (quality && clipped)
             atomicAdd(&result.audio.clipped, clipped);

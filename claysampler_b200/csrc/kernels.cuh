@@ -87,6 +87,32 @@ struct SegmentView {
     int blockCount;
 };
 
+// Quality-gate / group-volume inputs of one job (the reference's AudioJob,
+// src/cuda/render_types.h:116-118): frames of the melody body measured (0: none),
+// its first body window and first onset in the batch arrays, and its onset count.
+struct AssessJob {
+    int bodyFrames, bodyFirst, onsetFirst, onsetCount;
+};
+
+// Body windows are 250 ms (5 quality windows) restarting every 2 s
+// (src/cuda/quality.cu:13-19).
+struct BodyGeometry {
+    int chunk, span, perChunk;
+    __host__ __device__ int windowOf(int frame) const { return frame / chunk * perChunk + frame % chunk / span; }
+    __host__ __device__ int start(int window) const { return window / perChunk * chunk + window % perChunk * span; }
+    __host__ __device__ int windows(int frames) const      // windows covering [0, frames)
+    {
+        return frames / chunk * perChunk + (frames % chunk + span - 1) / span;
+    }
+};
+
+inline BodyGeometry bodyGeometry(const cs_audio_config& config)
+{
+    BodyGeometry g{2 * config.rate, 5 * config.window, 0};
+    g.perChunk = (g.chunk + g.span - 1) / g.span;
+    return g;
+}
+
 struct FinishView {
     StereoStats* stereo;
     MonoStats* windows;
@@ -94,6 +120,35 @@ struct FinishView {
     short* packed;
     cs_tail_result* results;
     int blockCount, windowCount;
+    // Body power per window, accumulated by finalizeKernel from the samples it
+    // writes (null when neither the quality gate nor group volume is on).
+    unsigned long long* bodyPower;
+    const AssessJob* assess;
+    BodyGeometry body;
+};
+
+// The assessment stage (src/cuda/quality.cu): onset levels, verdicts, group gains.
+struct AssessView {
+    const AssessJob* jobs;
+    const int* onsets;                  // onset frames, jobs concatenated
+    const int* onsetJob;                // job of each onset
+    const unsigned long long* bodyPower;
+    unsigned long long* onsetPower;     // loudest 50 ms window after each onset
+    cs_audio_config config;
+    BodyGeometry body;
+    int jobCount, onsetCount;
+};
+
+// Accepted-PCM packing (layoutAccepted + packAccepted, quality.cu:211-280): drops
+// rejected jobs, applies group gains and re-measures gained jobs.
+struct PackView {
+    const int* blockJob;                // job of each 1024-frame block
+    const int* jobBlockFirst;           // first block of each job
+    cs_tail_result* results;
+    uint64_t* sourceOffset;             // per job: its offset in `source` (set by the layout)
+    const short* source;
+    short* output;
+    int jobCount, blockCount;
 };
 
 void buildSincTable(float* phaseMajor);   // host: 2049 x 48 floats
@@ -106,5 +161,10 @@ int launchGeneralChains(const BatchView& b, const SegmentView& s, cudaStream_t s
 void launchMix(const BatchView& b, const SegmentView& s, bool natural, StereoStats* stats, cudaStream_t stream);
 int launchFinish(const BatchView& b, const FinishView& f, bool natural, bool quality, const TailConfig& tail,
                  cudaStream_t stream);
+// Onset levels (quality gate only) and per-job verdicts on the finished PCM.
+int launchMeasure(const AssessView& a, cs_tail_result* results, const short* pcm, bool natural, cudaStream_t stream);
+// Group gains for volume groups given as job ranges into `results`.
+int launchMatch(const int2* groups, int count, int minimum, cs_tail_result* results, cudaStream_t stream);
+int launchPack(const PackView& p, bool natural, cudaStream_t stream);
 
 } // namespace cs

@@ -63,11 +63,18 @@ struct HostBatch {
     std::vector<cs_voice_modulation> modulation;
     std::vector<JobInfo> jobs;
     std::vector<MixTile> tiles;
-    std::vector<int> indices, blockJob, windowJob, chainHeads, pitchHeads;
+    std::vector<int> indices, blockJob, windowJob, chainHeads, pitchHeads, jobBlockFirst;
     size_t frames = 0;
     int blocks = 0, windows = 0, lastFrame = 0;
+    // Quality gate / group volume inputs (src/cuda/renderer.cpp:801-842).
+    std::vector<AssessJob> assess;
+    std::vector<int> onsets, onsetJob;
+    std::vector<uint64_t> volumeGroups;
+    int bodyWindows = 0;
 
-    void append(const cs_plan& plan, int window, bool natural)
+    // `assessing`: the quality gate or group volume is on; `quality`: the gate is.
+    void append(const cs_plan& plan, int window, bool natural, bool assessing = false, bool quality = false,
+                const BodyGeometry& body = {1, 1, 1})
     {
         if (plan.track_count < 3)
             throw std::runtime_error("a plan needs its CC7, CC11 and CC10 tracks");
@@ -150,6 +157,20 @@ struct HostBatch {
             }
             voices.push_back(voice);
         }
+        if (assessing) {
+            const int bodyFrames = quality || plan.volume_group ? plan.body_frames : 0;
+            const int onsetCount = quality ? plan.onset_count : 0;
+            assess.push_back({bodyFrames, bodyWindows, int(onsets.size()), onsetCount});
+            for (int i = 0; i < onsetCount; ++i) {
+                if (plan.onsets[i] < 0)
+                    throw std::runtime_error("negative onset frame");
+                onsets.push_back(plan.onsets[i]);
+                onsetJob.push_back(int(jobs.size()));
+            }
+            bodyWindows += body.windows(bodyFrames);
+        }
+        volumeGroups.push_back(plan.volume_group);
+        jobBlockFirst.push_back(blocks);
         for (int b = 0; b < blockCount; ++b)
             blockJob.push_back(int(jobs.size()));
         for (int w = 0; w < windowCount; ++w)
@@ -396,6 +417,15 @@ struct cs_prepared {
     cudaEvent_t begin = nullptr, end = nullptr;
     std::vector<cs_tail_result> results;
     bool ran = false;
+    // Quality gate / group volume (null views when both are off).
+    bool assess = false;
+    bool deferGroups = false;           // a chunk of a volume group split across batches
+    cs::AssessView assessView{};
+    cs::PackView packView{};
+    std::vector<int2> groups;           // volume groups inside the batch, job ranges
+    const int2* deviceGroups = nullptr;
+    size_t bodyBytes = 0;
+    short* output = nullptr;            // the PCM the batch publishes
     // Optional per-stage timing: an event after every stage of the last run.
     bool profile = false;
     std::vector<cudaEvent_t> marks;
@@ -471,8 +501,23 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     p->owner = &r;
     p->natural = r.natural;
     HostBatch& batch = p->batch;
+    const bool assess = r.audio.enabled || r.groupMinimum > 0;
+    const BodyGeometry body = bodyGeometry(r.audio);
     for (size_t i = 0; i < count; ++i)
-        batch.append(plans[i], r.tail.window, r.natural);
+        batch.append(plans[i], r.tail.window, r.natural, assess, r.audio.enabled != 0, body);
+    p->assess = assess;
+    if (assess && r.groupMinimum > 0) {
+        // Volume groups: runs of equal nonzero ids (src/cuda/renderer.cpp:1751-1761).
+        const auto& ids = batch.volumeGroups;
+        for (size_t first = 0, end; first < ids.size(); first = end) {
+            end = first + 1;
+            if (!ids[first])
+                continue;
+            while (end < ids.size() && ids[end] == ids[first])
+                ++end;
+            p->groups.push_back(make_int2(int(first), int(end)));
+        }
+    }
     p->tables = planSegments(batch, r.scratchLimit ? r.scratchLimit : defaultScratchBudget());
     const SegmentTables& t = p->tables;
     const size_t jobs = batch.jobs.size();
@@ -497,6 +542,11 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     const size_t oSimple = section(t.simple.size() * sizeof(int));
     const size_t oPitch = section(t.pitch.size() * sizeof(int));
     const size_t oBlocks = section(t.blocks.size() * sizeof(int));
+    const size_t oJobBlockFirst = section(batch.jobBlockFirst.size() * sizeof(int));
+    const size_t oAssess = section(batch.assess.size() * sizeof(AssessJob));
+    const size_t oOnsets = section(batch.onsets.size() * sizeof(int));
+    const size_t oOnsetJob = section(batch.onsetJob.size() * sizeof(int));
+    const size_t oGroups = section(p->groups.size() * sizeof(int2));
     const size_t uploadEnd = layout.bytes;
     p->stateBytes = batch.voices.size() * sizeof(ChainState);
     const size_t oStates = section(p->stateBytes);
@@ -510,6 +560,10 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     const size_t oPacked = section(batch.frames * size_t(channels) * sizeof(short));
     const size_t oScratch = section(t.scratchBytes);
     const size_t oError = section(sizeof(int));
+    p->bodyBytes = size_t(batch.bodyWindows) * sizeof(unsigned long long);
+    const size_t oBodyPower = section(p->bodyBytes);
+    const size_t oOnsetPower = section(batch.onsets.size() * sizeof(unsigned long long));
+    const size_t oSourceOffset = section(assess ? jobs * sizeof(uint64_t) : 0);
     p->arenaBytes = layout.bytes;
 
     if (shared) {
@@ -567,6 +621,11 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     stage(oSimple, t.simple);
     stage(oPitch, t.pitch);
     stage(oBlocks, t.blocks);
+    stage(oJobBlockFirst, batch.jobBlockFirst);
+    stage(oAssess, batch.assess);
+    stage(oOnsets, batch.onsets);
+    stage(oOnsetJob, batch.onsetJob);
+    stage(oGroups, p->groups);
     check(cudaMemcpyAsync(base, staging, uploadEnd, cudaMemcpyHostToDevice, r.stream), "CUDA batch upload");
     check(cudaStreamSynchronize(r.stream), "CUDA batch upload");
 
@@ -618,13 +677,42 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     f.blockCount = batch.blocks;
     f.windowCount = batch.windows;
     p->stereo = f.stereo;
+    p->output = f.packed;
+    if (assess) {
+        f.bodyPower = reinterpret_cast<unsigned long long*>(base + oBodyPower);
+        f.assess = reinterpret_cast<const AssessJob*>(base + oAssess);
+        f.body = body;
+        AssessView& a = p->assessView;
+        a.jobs = f.assess;
+        a.onsets = reinterpret_cast<const int*>(base + oOnsets);
+        a.onsetJob = reinterpret_cast<const int*>(base + oOnsetJob);
+        a.bodyPower = f.bodyPower;
+        a.onsetPower = reinterpret_cast<unsigned long long*>(base + oOnsetPower);
+        a.config = r.audio;
+        a.body = body;
+        a.jobCount = int(jobs);
+        a.onsetCount = int(batch.onsets.size());
+        p->deviceGroups = reinterpret_cast<const int2*>(base + oGroups);
+        // Accepted PCM goes to a buffer that is dead once finishing is done: the
+        // mono quantisation (natural) or the PCM16 mix (orig/custom).
+        p->output = r.natural ? f.mono : static_cast<short*>(v.mix);
+        PackView& k = p->packView;
+        k.blockJob = v.blockJob;
+        k.jobBlockFirst = reinterpret_cast<const int*>(base + oJobBlockFirst);
+        k.results = f.results;
+        k.sourceOffset = reinterpret_cast<uint64_t*>(base + oSourceOffset);
+        k.source = f.packed;
+        k.output = p->output;
+        k.jobCount = int(jobs);
+        k.blockCount = batch.blocks;
+    }
     check(cudaEventCreate(&p->begin), "CUDA timing event");
     check(cudaEventCreate(&p->end), "CUDA timing event");
     return p.release();
 }
 
-const char* const kStageNames[] = {"pitch", "source", "recurrence", "general", "mix", "finish"};
-constexpr int kStages = 6;
+const char* const kStageNames[] = {"pitch", "source", "recurrence", "general", "mix", "finish", "assess"};
+constexpr int kStages = 7;
 
 void run(cs_renderer& r, cs_prepared& p, cudaStream_t stream)
 {
@@ -651,6 +739,8 @@ void run(cs_renderer& r, cs_prepared& p, cudaStream_t stream)
     check(cudaMemsetAsync(p.view.states, 0, std::max<size_t>(p.stateBytes, 1), stream), "CUDA state reset");
     check(cudaMemsetAsync(p.finish.results, 0, std::max<size_t>(p.resultBytes, 1), stream), "CUDA result reset");
     check(cudaMemsetAsync(p.view.error, 0, sizeof(int), stream), "CUDA error flag reset");
+    if (p.bodyBytes)
+        check(cudaMemsetAsync(p.finish.bodyPower, 0, p.bodyBytes, stream), "CUDA body power reset");
     stage(-1);
     for (size_t i = 0; i < p.segments.size(); ++i) {
         BatchView view = p.view;
@@ -675,6 +765,20 @@ void run(cs_renderer& r, cs_prepared& p, cudaStream_t stream)
     launches += launchFinish(p.view, p.finish, r.natural, r.audio.enabled != 0, r.tail, stream);
     stage(5);
     check(cudaGetLastError(), "CUDA finishing launch");
+    if (p.assess) {
+        // Quality gate and group volume (src/cuda/renderer.cpp:1170-1180, 1134-1148):
+        // verdicts, then the gains of the groups the batch holds whole, then the
+        // accepted PCM.  A chunk of a split group stops after the verdicts; its
+        // caller matches the whole group and packs each chunk.
+        launches += launchMeasure(p.assessView, p.finish.results, p.finish.packed, r.natural, stream);
+        if (!p.deferGroups) {
+            if (r.groupMinimum > 0)
+                launches += launchMatch(p.deviceGroups, int(p.groups.size()), r.groupMinimum, p.finish.results, stream);
+            launches += launchPack(p.packView, r.natural, stream);
+        }
+        stage(6);
+        check(cudaGetLastError(), "CUDA assessment launch");
+    }
     check(cudaEventRecord(p.end, stream), "CUDA timing record");
     p.launches = launches;
     p.ran = true;
@@ -720,6 +824,326 @@ int guarded(F&& body)
         return 1;
     }
 }
+
+
+// Renderer::renderWindow (src/cuda/renderer.cpp:1748-1820) over staged batches.
+// Batches take up to batchJobs plans and never cut a volume group unless the group
+// alone exceeds a batch; such a group is rendered in chunks whose accepted PCM
+// waits on the device (within the waiting limit) or in host memory until the last
+// chunk's verdicts are in, then every chunk is packed with the group's gains
+// (finishSplit, retain and packRetained, renderer.cpp:1206-1346).
+class WindowRenderer {
+public:
+    WindowRenderer(cs_renderer& renderer, cs_publish_fn publish, cs_refill_fn refill, void* user)
+        : r(renderer), publish(publish), refill(refill), user(user) {}
+
+    void render(const cs_plan* plans, size_t count)
+    {
+        queue.assign(plans, plans + count);
+        size_t first = 0;
+        for (;;) {
+            if (first == queue.size()) {
+                const cs_plan* more = nullptr;
+                size_t moreCount = 0;
+                if (!refill || !refill(user, 1, &more, &moreCount) || !moreCount)
+                    break;
+                checkPlans(more, moreCount);
+                queue.insert(queue.end(), more, more + moreCount);
+            }
+            size_t jobs = batchEnd(first, std::min(queue.size(), first + r.batchJobs)) - first;
+            cs_prepared* prepared = nullptr;
+            for (;;) {
+                try {
+                    prepared = prepare(r, queue.data() + first, jobs, true);
+                    break;
+                } catch (const CudaError& e) {
+                    if (e.code != cudaErrorMemoryAllocation)
+                        throw;
+                    // Allocation recovery: retry with half the jobs, then reject the
+                    // single job (src/cuda/renderer.cpp:947-992).
+                    if (jobs > 1) {
+                        jobs = batchEnd(first, first + jobs / 2) - first;
+                        continue;
+                    }
+                    break;
+                }
+            }
+            if (!prepared) {
+                rejectScratch(first);
+                // A split group whose last member was rejected still publishes the
+                // members it retained.
+                const uint64_t id = queue[first].volume_group;
+                if (!chunks.empty() && !(first + 1 < queue.size() && id && queue[first + 1].volume_group == id))
+                    finishGroup(nullptr, first);
+                first += 1;
+                continue;
+            }
+            std::unique_ptr<cs_prepared, void (*)(cs_prepared*)> guard(prepared, cs_prepared_destroy);
+            const uint64_t id = queue[first].volume_group;
+            const bool continues = first + jobs < queue.size() && id && queue[first + jobs].volume_group == id;
+            const bool split = r.groupMinimum > 0 && id && (continues || (first > 0 && queue[first - 1].volume_group == id));
+            if (!split) {
+                run(r, *prepared, nullptr);
+                publishBatch(*prepared, first);
+            } else {
+                prepared->deferGroups = true;
+                run(r, *prepared, nullptr);
+                if (continues)
+                    retainChunk(*prepared, first);
+                else
+                    finishGroup(prepared, first);
+            }
+            first += jobs;
+        }
+    }
+
+private:
+    struct Chunk {
+        size_t first = 0;
+        std::vector<int> blockJob, jobBlockFirst;
+        std::vector<cs_tail_result> results;   // after the chunk's own acceptance layout
+        size_t samples = 0;
+        void* device = nullptr;                 // waiting on the device
+        std::vector<int16_t> host;              // spilled to host memory
+        double seconds = 0;
+    };
+
+    cs_renderer& r;
+    cs_publish_fn publish;
+    cs_refill_fn refill;
+    void* user;
+    std::vector<cs_plan> queue;
+    std::vector<Chunk> chunks;                  // the split group rendered so far
+
+    // End of a batch [first, end): stops before a volume group the batch would cut
+    // (unless the batch starts with it) and at the end of a split group it continues
+    // (trySynthesize's group rule, src/cuda/renderer.cpp:816-829).
+    size_t batchEnd(size_t first, size_t end) const
+    {
+        if (r.groupMinimum <= 0 || end <= first)
+            return end;
+        const uint64_t head = queue[first].volume_group;
+        if (head && first > 0 && queue[first - 1].volume_group == head) {
+            size_t stop = first;
+            while (stop < end && queue[stop].volume_group == head)
+                ++stop;
+            return stop;
+        }
+        if (end < queue.size()) {
+            const uint64_t id = queue[end - 1].volume_group;
+            if (id && queue[end].volume_group == id) {
+                size_t start = end - 1;
+                while (start > first && queue[start - 1].volume_group == id)
+                    --start;
+                if (start > first)
+                    return start;
+            }
+        }
+        return end;
+    }
+
+    double seconds(cs_prepared& p)
+    {
+        float ms = 0;
+        check(cudaEventElapsedTime(&ms, p.begin, p.end), "CUDA kernel timing");
+        return ms / 1000.0;
+    }
+
+    void rejectScratch(size_t first)
+    {
+        cs_batch rejected{};
+        rejected.failed_scratch_bytes = 1;
+        publish(user, &rejected, first);
+    }
+
+    void deliver(const int16_t* pcm, size_t samples, const cs_tail_result* results, size_t count, double kernel,
+                 size_t first)
+    {
+        r.downloaded += samples * sizeof(int16_t);
+        cs_batch batch{};
+        batch.pcm = pcm;
+        batch.pcm_samples = samples;
+        batch.results = results;
+        batch.result_count = count;
+        batch.kernel_seconds = kernel;
+        publish(user, &batch, first);
+    }
+
+    int16_t* hostPcm(size_t samples)
+    {
+        return static_cast<int16_t*>(cs_renderer::pinned(r.hostPcm, r.hostPcmCapacity,
+                                                         std::max<size_t>(samples, 1) * sizeof(int16_t)));
+    }
+
+    void publishBatch(cs_prepared& p, size_t first)
+    {
+        const size_t samples = collectResults(r, p);
+        int16_t* pcm = hostPcm(samples);
+        if (samples)
+            check(cudaMemcpy(pcm, p.output, samples * sizeof(int16_t), cudaMemcpyDeviceToHost), "CUDA PCM download");
+        deliver(pcm, samples, p.results.data(), p.results.size(), seconds(p), first);
+    }
+
+    static size_t samplesOf(const std::vector<cs_tail_result>& results, int channels)
+    {
+        if (results.empty())
+            return 0;
+        return size_t(results.back().offset + uint64_t(results.back().dataFrames)) * size_t(channels);
+    }
+
+    // A chunk that is not the group's last: pack its accepted PCM without gains and
+    // keep it (retain, src/cuda/renderer.cpp:1202-1236).
+    void retainChunk(cs_prepared& p, size_t first)
+    {
+        check(cudaStreamSynchronize(r.stream), "CUDA chunk verdicts");
+        const int channels = r.natural ? 1 : 2;
+        launchPack(p.packView, r.natural, r.stream);
+        check(cudaGetLastError(), "CUDA chunk packing launch");
+        check(cudaEventRecord(p.end, r.stream), "CUDA timing record");
+        collectResults(r, p);
+        Chunk chunk;
+        chunk.first = first;
+        chunk.blockJob = p.batch.blockJob;
+        chunk.jobBlockFirst = p.batch.jobBlockFirst;
+        chunk.results = p.results;
+        chunk.samples = samplesOf(p.results, channels);
+        chunk.seconds = seconds(p);
+        const size_t bytes = chunk.samples * sizeof(int16_t);
+        if (bytes) {
+            size_t freeBytes = 0, total = 0;
+            check(cudaMemGetInfo(&freeBytes, &total), "CUDA waiting memory budget");
+            const size_t limit = std::min(r.waitingLimit, total / 16);
+            if (r.waiting <= limit && bytes <= std::min(limit - r.waiting, freeBytes / 4)) {
+                if (cudaMalloc(&chunk.device, bytes) == cudaSuccess) {
+                    r.waiting += bytes;
+                    r.peakWaiting = std::max(r.peakWaiting, r.waiting);
+                    r.live += bytes;
+                    r.record();
+                    check(cudaMemcpy(chunk.device, p.output, bytes, cudaMemcpyDeviceToDevice), "CUDA retain group PCM");
+                } else {
+                    cudaGetLastError();
+                    chunk.device = nullptr;
+                }
+            }
+            if (!chunk.device) {
+                chunk.host.resize(chunk.samples);
+                check(cudaMemcpy(chunk.host.data(), p.output, bytes, cudaMemcpyDeviceToHost), "CUDA spill group PCM");
+                r.spilled += bytes;
+            }
+        }
+        chunks.push_back(std::move(chunk));
+    }
+
+    // The group's last chunk: match the whole group's gains, pack and publish this
+    // chunk (none when its job was rejected), then pack and publish every retained
+    // chunk.
+    void finishGroup(cs_prepared* p, size_t first)
+    {
+        const int channels = r.natural ? 1 : 2;
+        std::vector<cs_tail_result> group;
+        for (const Chunk& c : chunks)
+            group.insert(group.end(), c.results.begin(), c.results.end());
+        const size_t local = group.size();
+        if (p) {
+            collectResults(r, *p);
+            group.insert(group.end(), p->results.begin(), p->results.end());
+        }
+        const size_t resultBytes = std::max<size_t>(group.size(), 1) * sizeof(cs_tail_result);
+        void* control = nullptr;
+        check(cudaMalloc(&control, resultBytes + sizeof(int2)), "CUDA group control allocation");
+        std::unique_ptr<void, cudaError_t (*)(void*)> controlGuard(control, cudaFree);
+        auto* results = static_cast<cs_tail_result*>(control);
+        auto* range = reinterpret_cast<int2*>(static_cast<unsigned char*>(control) + resultBytes);
+        const int2 whole = make_int2(0, int(group.size()));
+        if (!group.empty())
+            check(cudaMemcpy(results, group.data(), group.size() * sizeof(cs_tail_result), cudaMemcpyHostToDevice),
+                  "CUDA group metadata upload");
+        check(cudaMemcpy(range, &whole, sizeof whole, cudaMemcpyHostToDevice), "CUDA group upload");
+        launchMatch(range, 1, r.groupMinimum, results, r.stream);
+        double kernel = 0;
+        for (const Chunk& c : chunks)
+            kernel += c.seconds;
+        if (p) {
+            PackView view = p->packView;
+            view.results = results + local;
+            launchPack(view, r.natural, r.stream);
+            check(cudaGetLastError(), "CUDA group packing launch");
+            check(cudaStreamSynchronize(r.stream), "CUDA group packing");
+            std::vector<cs_tail_result> mine(p->results.size());
+            check(cudaMemcpy(mine.data(), view.results, mine.size() * sizeof(cs_tail_result),
+                             cudaMemcpyDeviceToHost), "CUDA render metadata download");
+            const size_t samples = samplesOf(mine, channels);
+            int16_t* pcm = hostPcm(samples);
+            if (samples)
+                check(cudaMemcpy(pcm, p->output, samples * sizeof(int16_t), cudaMemcpyDeviceToHost),
+                      "CUDA PCM download");
+            deliver(pcm, samples, mine.data(), mine.size(), kernel + seconds(*p), first);
+            kernel = 0;
+        } else {
+            check(cudaGetLastError(), "CUDA group volume launch");
+        }
+        size_t at = 0;
+        for (Chunk& c : chunks) {
+            packRetained(c, results + at, kernel);
+            kernel = 0;
+            at += c.results.size();
+        }
+        chunks.clear();
+    }
+
+    // packRetained (src/cuda/renderer.cpp:1238-1279): the chunk's waiting PCM with
+    // the matched results.
+    void packRetained(Chunk& c, cs_tail_result* results, double kernel)
+    {
+        const int channels = r.natural ? 1 : 2;
+        const size_t jobs = c.results.size(), blocks = c.blockJob.size();
+        const size_t bytes = c.samples * sizeof(int16_t);
+        Layout layout;
+        const size_t oBlockJob = layout.add(std::max<size_t>(blocks * sizeof(int), 1));
+        const size_t oJobBlock = layout.add(std::max<size_t>(jobs * sizeof(int), 1));
+        const size_t oSource = layout.add(std::max<size_t>(jobs * sizeof(uint64_t), 1));
+        const size_t oSpill = layout.add(c.device ? 1 : std::max<size_t>(bytes, 1));
+        const size_t oOutput = layout.add(std::max<size_t>(bytes, 1));
+        void* arena = nullptr;
+        check(cudaMalloc(&arena, layout.bytes), "CUDA retained group scratch allocation");
+        std::unique_ptr<void, cudaError_t (*)(void*)> arenaGuard(arena, cudaFree);
+        auto* base = static_cast<unsigned char*>(arena);
+        check(cudaMemcpy(base + oBlockJob, c.blockJob.data(), blocks * sizeof(int), cudaMemcpyHostToDevice),
+              "CUDA retained job upload");
+        check(cudaMemcpy(base + oJobBlock, c.jobBlockFirst.data(), jobs * sizeof(int), cudaMemcpyHostToDevice),
+              "CUDA retained job upload");
+        if (!c.device && bytes)
+            check(cudaMemcpy(base + oSpill, c.host.data(), bytes, cudaMemcpyHostToDevice), "CUDA spilled PCM upload");
+        PackView view{};
+        view.blockJob = reinterpret_cast<const int*>(base + oBlockJob);
+        view.jobBlockFirst = reinterpret_cast<const int*>(base + oJobBlock);
+        view.results = results;
+        view.sourceOffset = reinterpret_cast<uint64_t*>(base + oSource);
+        view.source = static_cast<const short*>(c.device ? c.device : static_cast<void*>(base + oSpill));
+        view.output = reinterpret_cast<short*>(base + oOutput);
+        view.jobCount = int(jobs);
+        view.blockCount = int(blocks);
+        launchPack(view, r.natural, r.stream);
+        check(cudaGetLastError(), "CUDA retained packing launch");
+        check(cudaStreamSynchronize(r.stream), "CUDA retained packing");
+        std::vector<cs_tail_result> packed(jobs);
+        check(cudaMemcpy(packed.data(), results, jobs * sizeof(cs_tail_result), cudaMemcpyDeviceToHost),
+              "CUDA retained job metadata download");
+        const size_t samples = samplesOf(packed, channels);
+        int16_t* pcm = hostPcm(samples);
+        if (samples)
+            check(cudaMemcpy(pcm, view.output, samples * sizeof(int16_t), cudaMemcpyDeviceToHost),
+                  "CUDA PCM download");
+        if (c.device) {
+            cudaFree(c.device);
+            c.device = nullptr;
+            r.waiting -= bytes;
+            r.live -= bytes;
+        }
+        c.host.clear();
+        deliver(pcm, samples, packed.data(), packed.size(), kernel, c.first);
+    }
+};
 
 } // namespace
 } // namespace cs
@@ -854,7 +1278,7 @@ int cs_collect(cs_renderer* r, cs_prepared* p, int16_t* pcm, size_t capacity, si
             if (capacity < count)
                 throw std::runtime_error("PCM buffer too small");
             if (count)
-                cs::check(cudaMemcpy(pcm, p->finish.packed, count * sizeof(int16_t), cudaMemcpyDeviceToHost),
+                cs::check(cudaMemcpy(pcm, p->output, count * sizeof(int16_t), cudaMemcpyDeviceToHost),
                           "CUDA PCM download");
             r->downloaded += count * sizeof(int16_t);
         }
@@ -931,63 +1355,8 @@ int cs_render_window(cs_renderer* r, const cs_plan* plans, size_t count, cs_publ
     return cs::guarded([&] {
         if (!r || !publish)
             throw std::runtime_error("null renderer or publish callback");
-        std::vector<cs_plan> queue(plans, plans + count);
         cs::checkPlans(plans, count);
-        size_t first = 0;
-        for (;;) {
-            if (first == queue.size()) {
-                const cs_plan* more = nullptr;
-                size_t moreCount = 0;
-                if (!refill || !refill(user, 1, &more, &moreCount) || !moreCount)
-                    break;
-                cs::checkPlans(more, moreCount);
-                queue.insert(queue.end(), more, more + moreCount);
-            }
-            size_t jobs = std::min(r->batchJobs, queue.size() - first);
-            cs_prepared* prepared = nullptr;
-            for (;;) {
-                try {
-                    prepared = cs::prepare(*r, queue.data() + first, jobs, true);
-                    break;
-                } catch (const cs::CudaError& e) {
-                    if (e.code != cudaErrorMemoryAllocation)
-                        throw;
-                    // Allocation recovery: retry with half the jobs, then reject the
-                    // single job (src/cuda/renderer.cpp:947-992).
-                    if (jobs > 1) {
-                        jobs /= 2;
-                        continue;
-                    }
-                    break;
-                }
-            }
-            if (!prepared) {
-                cs_batch rejected{};
-                rejected.failed_scratch_bytes = 1;
-                publish(user, &rejected, first);
-                first += 1;
-                continue;
-            }
-            std::unique_ptr<cs_prepared, void (*)(cs_prepared*)> guard(prepared, cs_prepared_destroy);
-            cs::run(*r, *prepared, nullptr);
-            const size_t samples = cs::collectResults(*r, *prepared);
-            auto* pcm = static_cast<int16_t*>(
-                cs_renderer::pinned(r->hostPcm, r->hostPcmCapacity, std::max<size_t>(samples, 1) * sizeof(int16_t)));
-            if (samples)
-                cs::check(cudaMemcpy(pcm, prepared->finish.packed, samples * sizeof(int16_t),
-                                     cudaMemcpyDeviceToHost), "CUDA PCM download");
-            r->downloaded += samples * sizeof(int16_t);
-            float ms = 0;
-            cs::check(cudaEventElapsedTime(&ms, prepared->begin, prepared->end), "CUDA kernel timing");
-            cs_batch batch{};
-            batch.pcm = pcm;
-            batch.pcm_samples = samples;
-            batch.results = prepared->results.data();
-            batch.result_count = prepared->results.size();
-            batch.kernel_seconds = ms / 1000.0;
-            publish(user, &batch, first);
-            first += jobs;
-        }
+        cs::WindowRenderer(*r, publish, refill, user).render(plans, count);
     });
 }
 

@@ -42,6 +42,11 @@ def lib() -> ctypes.CDLL:
         _lib.oracle_finish_stereo.argtypes = [vp, vp, i32, i32, vp, vp]
         if hasattr(_lib, "oracle_synthesize"):
             _lib.oracle_synthesize.argtypes = [vp, i32, vp, i32, i32, vp]
+        _lib.oracle_assess.restype = ctypes.c_size_t
+        _lib.oracle_assess.argtypes = [vp, i32, vp, i32, vp, i32, vp, vp]
+        _lib.oracle_match_group.argtypes = [vp, i32, i32]
+        _lib.oracle_pack_accepted.restype = ctypes.c_size_t
+        _lib.oracle_pack_accepted.argtypes = [vp, i32, vp, i32, vp, vp]
     return _lib
 
 
@@ -72,3 +77,18 @@ def synthesize(plans: list[Plan], bank: np.ndarray, natural: bool = True, thread
     lib().oracle_synthesize(array, len(plans), bank.ctypes.data if bank.size else None, int(natural),
                             threads or os.cpu_count() or 1, out.ctypes.data)
     return out
+
+
+def assess(finished: np.ndarray, results: np.ndarray, plans: list[Plan], natural: bool = True, config=None,
+           group_minimum: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """(accepted PCM16, results) of the reference's quality gate, group volume and
+    accepted packing (src/cuda/quality.cu) applied to a finished batch."""
+    from claysampler_b200.plans import default_audio_config
+    config = default_audio_config() if config is None else np.asarray(config)
+    finished = np.ascontiguousarray(finished, np.int16)
+    out = np.array(results, TAIL_RESULT, copy=True)
+    accepted = np.zeros(max(finished.size, 1), np.int16)
+    array = c_plans(plans)
+    n = lib().oracle_assess(finished.ctypes.data, 1 if natural else 2, array, len(plans), config.ctypes.data,
+                            group_minimum, out.ctypes.data, accepted.ctypes.data)
+    return accepted[:n], out
