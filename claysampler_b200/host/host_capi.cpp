@@ -158,6 +158,16 @@ int cs_host_plan(cs_host* host, const char* sfz, const char* midiPath, int rate,
     });
 }
 
+int cs_host_check_sfz(const char* sfz, int* regions)
+{
+    return guarded([&] {
+        if (!sfz || !regions)
+            throw std::runtime_error("null argument");
+        csh::SampleBank bank;
+        *regions = int(csh::loadInstrument(sfz, bank).regions.size());
+    });
+}
+
 int cs_host_bank(cs_host* host, const float** pcm, size_t* floats)
 {
     return guarded([&] {

@@ -34,6 +34,10 @@ int cs_host_plan(cs_host* host, const char* sfz, const char* midi, int rate, int
                  void** image, size_t* size);
 void cs_host_free(void* pointer);
 
+/* Loads one SFZ preset with a private bank and reports its region count: the
+ * reference CLI's --check-sfz (src/main.cpp:264-287). */
+int cs_host_check_sfz(const char* sfz, int* regions);
+
 /* The shared decoded bank (AudioBank::pcm, src/io/audio.h:32); valid until the
  * next cs_host_plan or cs_host_release_bank. */
 int cs_host_bank(cs_host* host, const float** pcm, size_t* floats);
