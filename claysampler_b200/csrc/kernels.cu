@@ -321,127 +321,6 @@ __global__ void __launch_bounds__(kSourceTile) sourceKernel(BatchView b, Segment
     }
 }
 
-struct RecurrenceState {
-    Compact c;
-    float z1l[3], z2l[3], z1r[3], z2r[3];
-};
-
-template <bool Stereo>
-__device__ __forceinline__ void cascade(float& x, float& y, const Biquad& q, int sections, RecurrenceState& st)
-{
-    #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        if (k < sections) {
-            x = biquadStep(x, q, st.z1l[k], st.z2l[k]);
-            if (Stereo)
-                y = biquadStep(y, q, st.z1r[k], st.z2r[k]);
-        }
-    }
-}
-
-// One span of one chain: smoothing + cascade over frames [0, n) in place.
-template <bool Stereo>
-__device__ __forceinline__ void runSpan(float* src, const float* tgt, int n, int type, int sections, bool moving,
-                                        float amount, bool& initialized, RecurrenceState& st)
-{
-    constexpr int ch = Stereo ? 2 : 1;
-    const auto step = [&](float& x, float& y, float t0, float t1, float t2, bool haveTarget) {
-        if (haveTarget) {
-            if (initialized) {
-                st.c.c0 = fmaf(amount, t0 - st.c.c0, st.c.c0);
-                st.c.c1 = fmaf(amount, t1 - st.c.c1, st.c.c1);
-                st.c.c2 = fmaf(amount, t2 - st.c.c2, st.c.c2);
-            } else {
-                st.c = {t0, t1, t2};
-            }
-        }
-        initialized = true;
-        const Biquad q = expand(type, st.c);
-        cascade<Stereo>(x, y, q, sections, st);
-    };
-    int i = 0;
-    if (moving && sections) {
-        for (; i + 4 <= n; i += 4) {
-            float xs[4], ys[4];
-            if (Stereo) {
-                const float4 a = *reinterpret_cast<const float4*>(src + 2 * i);
-                const float4 c = *reinterpret_cast<const float4*>(src + 2 * i + 4);
-                xs[0] = a.x; ys[0] = a.y; xs[1] = a.z; ys[1] = a.w;
-                xs[2] = c.x; ys[2] = c.y; xs[3] = c.z; ys[3] = c.w;
-            } else {
-                const float4 a = *reinterpret_cast<const float4*>(src + i);
-                xs[0] = a.x; xs[1] = a.y; xs[2] = a.z; xs[3] = a.w;
-                ys[0] = ys[1] = ys[2] = ys[3] = 0.f;
-            }
-            const float4 t0 = *reinterpret_cast<const float4*>(tgt + 3 * i);
-            const float4 t1 = *reinterpret_cast<const float4*>(tgt + 3 * i + 4);
-            const float4 t2 = *reinterpret_cast<const float4*>(tgt + 3 * i + 8);
-            step(xs[0], ys[0], t0.x, t0.y, t0.z, true);
-            step(xs[1], ys[1], t0.w, t1.x, t1.y, true);
-            step(xs[2], ys[2], t1.z, t1.w, t2.x, true);
-            step(xs[3], ys[3], t2.y, t2.z, t2.w, true);
-            if (Stereo) {
-                *reinterpret_cast<float4*>(src + 2 * i) = make_float4(xs[0], ys[0], xs[1], ys[1]);
-                *reinterpret_cast<float4*>(src + 2 * i + 4) = make_float4(xs[2], ys[2], xs[3], ys[3]);
-            } else {
-                *reinterpret_cast<float4*>(src + i) = make_float4(xs[0], xs[1], xs[2], xs[3]);
-            }
-        }
-        for (; i < n; ++i) {
-            float x = src[ch * i], y = Stereo ? src[ch * i + 1] : 0.f;
-            step(x, y, tgt[3 * i], tgt[3 * i + 1], tgt[3 * i + 2], true);
-            src[ch * i] = x;
-            if (Stereo) src[ch * i + 1] = y;
-        }
-        return;
-    }
-    if (i < n && sections && !initialized) {
-        float x = src[0], y = Stereo ? src[1] : 0.f;
-        step(x, y, tgt[0], tgt[1], tgt[2], true);
-        src[0] = x;
-        if (Stereo) src[1] = y;
-        i = 1;
-    }
-    initialized = initialized || n > 0;
-    if (!sections)
-        return;
-    const Biquad q = expand(type, st.c);
-    for (; i < n && (i & 3); ++i) {
-        float x = src[ch * i], y = Stereo ? src[ch * i + 1] : 0.f;
-        cascade<Stereo>(x, y, q, sections, st);
-        src[ch * i] = x;
-        if (Stereo) src[ch * i + 1] = y;
-    }
-    for (; i + 4 <= n; i += 4) {
-        float xs[4], ys[4];
-        if (Stereo) {
-            const float4 a = *reinterpret_cast<const float4*>(src + 2 * i);
-            const float4 c = *reinterpret_cast<const float4*>(src + 2 * i + 4);
-            xs[0] = a.x; ys[0] = a.y; xs[1] = a.z; ys[1] = a.w;
-            xs[2] = c.x; ys[2] = c.y; xs[3] = c.z; ys[3] = c.w;
-        } else {
-            const float4 a = *reinterpret_cast<const float4*>(src + i);
-            xs[0] = a.x; xs[1] = a.y; xs[2] = a.z; xs[3] = a.w;
-            ys[0] = ys[1] = ys[2] = ys[3] = 0.f;
-        }
-        #pragma unroll
-        for (int k = 0; k < 4; ++k)
-            cascade<Stereo>(xs[k], ys[k], q, sections, st);
-        if (Stereo) {
-            *reinterpret_cast<float4*>(src + 2 * i) = make_float4(xs[0], ys[0], xs[1], ys[1]);
-            *reinterpret_cast<float4*>(src + 2 * i + 4) = make_float4(xs[2], ys[2], xs[3], ys[3]);
-        } else {
-            *reinterpret_cast<float4*>(src + i) = make_float4(xs[0], xs[1], xs[2], xs[3]);
-        }
-    }
-    for (; i < n; ++i) {
-        float x = src[ch * i], y = Stereo ? src[ch * i + 1] : 0.f;
-        cascade<Stereo>(x, y, q, sections, st);
-        src[ch * i] = x;
-        if (Stereo) src[ch * i + 1] = y;
-    }
-}
-
 // ---- TMA-staged serial recurrences --------------------------------------------------
 //
 // Lane = chain.  Each lane keeps two 32-frame chunks of its chain in shared memory,
@@ -671,7 +550,7 @@ __device__ __forceinline__ void advanceRun(const BatchView& b, const SegmentView
         r = enterRun(b, s, b.voices[r.span].nextFilteredSpan, fslot);
 }
 
-__global__ void __launch_bounds__(kRecThreads) recurrenceKernel(BatchView b, SegmentView s, int* error)
+__global__ void __launch_bounds__(kRecThreads, 1) recurrenceKernel(BatchView b, SegmentView s, int* error)
 {
     extern __shared__ __align__(16) unsigned char staged[];
     __shared__ __align__(8) uint64_t bars[kRecWarps * kRecChains][kRecBuffers];
@@ -757,8 +636,10 @@ __global__ void __launch_bounds__(kRecThreads) recurrenceKernel(BatchView b, Seg
                 initialized = true;
                 const Biquad q = expand(type, c);
                 float x = frames[channel];
-                for (int k = 0; k < sections; ++k)
-                    x = biquadStep(x, q, z1[k], z2[k]);
+                #pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    if (k < sections)
+                        x = biquadStep(x, q, z1[k], z2[k]);
                 out[0] = x;
                 first = 1;
             }

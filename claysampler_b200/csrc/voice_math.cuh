@@ -28,17 +28,54 @@ __device__ __forceinline__ float envelopeAt(const Shape& e, int frame)
     return fmaxf(e.sustain, expf(float(frame - e.decayStart + 1) * e.decayRate));
 }
 
-// Piecewise-linear track value: the last point with point.frame <= frame in
-// [low, high) (render.cu:107-118).
+#ifndef CS_TRACK_WINDOW
+#define CS_TRACK_WINDOW 4
+#endif
+
+// Binary search for the last point with point.frame <= frame in [below, above),
+// given points[below].frame <= frame < points[above].frame.
+__device__ __forceinline__ int searchPoints(const cs_control_point* __restrict__ points, int below, int above, int frame)
+{
+    while (below + 1 < above) {
+        const int mid = below + (above - below) / 2;
+        if (__ldg(&points[mid].frame) <= frame) below = mid;
+        else above = mid;
+    }
+    return below;
+}
+
+// Index of the last point with point.frame <= frame in [low, high) of a track whose
+// frames do not decrease, or `low` when there is none: the point the reference's
+// binary search lands on (render.cu:107-118).  Past the track's first point, a
+// guess interpolated between its second and last points (right or off by one for
+// evenly spaced points, such as an LFO baked every 16 frames after its start
+// anchor) bounds a window of 2 x CS_TRACK_WINDOW points; when the window holds the
+// answer the search takes a few steps inside it, otherwise it falls back to the
+// whole track.  Either way the index is the one the binary search finds.
+__device__ __forceinline__ int pointAt(const cs_control_point* __restrict__ points, int low, int high, int frame)
+{
+    if (high - low <= 1)
+        return low;
+    const int second = low + 1;
+    const int secondFrame = __ldg(&points[second].frame), lastFrame = __ldg(&points[high - 1].frame);
+    if (frame >= lastFrame)
+        return high - 1;
+    if (frame < secondFrame)
+        return low;                     // whether or not the first point is due
+    // secondFrame <= frame < lastFrame: the answer lies in [second, high - 2].
+    const float scale = __fdividef(float(high - 1 - second), float(lastFrame - secondFrame));
+    const int guess = second + __float2int_rz(float(frame - secondFrame) * scale);
+    const int below = max(second, guess - CS_TRACK_WINDOW), above = min(high - 1, guess + CS_TRACK_WINDOW);
+    if (below < above && __ldg(&points[below].frame) <= frame && __ldg(&points[above].frame) > frame)
+        return searchPoints(points, below, above, frame);
+    return searchPoints(points, second, high - 1, frame);
+}
+
+// Piecewise-linear track value at the point pointAt finds (render.cu:107-118).
 __device__ __forceinline__ float trackAt(const cs_control_point* __restrict__ points, int low, int high, int frame)
 {
-    while (low + 1 < high) {
-        const int mid = low + (high - low) / 2;
-        if (__ldg(&points[mid].frame) <= frame) low = mid;
-        else high = mid;
-    }
-    const int at = __ldg(&points[low].frame);
-    return fmaf(__ldg(&points[low].step), float(frame - at), __ldg(&points[low].value));
+    const int at = pointAt(points, low, high, frame);
+    return fmaf(__ldg(&points[at].step), float(frame - __ldg(&points[at].frame)), __ldg(&points[at].value));
 }
 
 __device__ __forceinline__ float bindingAt(const cs_voice_modulation& m, const cs_control_point* __restrict__ points,
@@ -191,51 +228,51 @@ __device__ __forceinline__ float2 panGains(const cs_voice_span& v, float offset)
     return make_float2(v.gain * cosf((1 + p) * kQuarterPi), v.gain * cosf((1 - p) * kQuarterPi));
 }
 
-// Enveloped, modulated, panned voice frame (render.cu:138-187).  With
-// `filterInput`, mono sources are returned before panning (the mix pans them
-// after the filter).
-__device__ __forceinline__ float2 voiceFrame(const float* __restrict__ bank, const float* __restrict__ sinc,
-                                             const cs_voice_span& v, const cs_control_point* __restrict__ points,
-                                             const cs_voice_modulation* __restrict__ modulation, float pan,
-                                             int frame, bool filterInput, double phase)
+// Modulation sums of one voice frame (render.cu:138-160): the enveloped level times
+// the amplitude bindings, and the sums of the volume (dB), pan, width and
+// position bindings, each accumulated in binding order.
+struct VoiceMods {
+    float level, db, pan, width, position;
+};
+
+__device__ __forceinline__ void addVoiceMod(VoiceMods& s, int target, float value)
 {
-    float level = envelopeAt(v, frame);
-    if (level <= 0)
-        return make_float2(0.f, 0.f);
-    float db = 0, widthOffset = 0, positionOffset = 0;
-    const int modEnd = v.firstModulation + v.modulationCount;
-    for (int j = v.firstModulation; j < modEnd; ++j) {
-        const cs_voice_modulation m = modulation[j];
-        if (m.target > CS_MOD_POSITION)
-            continue;
-        const float value = bindingAt(m, points, frame);
-        switch (m.target) {
-        case CS_MOD_AMPLITUDE: level *= value; break;
-        case CS_MOD_VOLUME: db += value; break;
-        case CS_MOD_PAN: pan += value; break;
-        case CS_MOD_WIDTH: widthOffset += value; break;
-        case CS_MOD_POSITION: positionOffset += value; break;
-        default: break;
-        }
+    switch (target) {
+    case CS_MOD_AMPLITUDE: s.level *= value; break;
+    case CS_MOD_VOLUME: s.db += value; break;
+    case CS_MOD_PAN: s.pan += value; break;
+    case CS_MOD_WIDTH: s.width += value; break;
+    case CS_MOD_POSITION: s.position += value; break;
+    default: break;
     }
-    if (db != 0)
-        level *= exp2f(db * .166096404744368f);
+}
+
+// The voice frame from its modulation sums (render.cu:160-187).  With
+// `filterInput`, mono sources are returned before panning (the mix pans them after
+// the filter).
+__device__ __forceinline__ float2 voiceOutput(const float* __restrict__ bank, const float* __restrict__ sinc,
+                                              const cs_voice_span& v, const VoiceMods& s, int frame,
+                                              bool filterInput, double phase)
+{
+    float level = s.level;
+    if (s.db != 0)
+        level *= exp2f(s.db * .166096404744368f);
     const float2 sample = voiceSource(bank, sinc, v, frame, phase);
     if (filterInput && v.channels == 1)
         return make_float2(sample.x * level, sample.x * level);
-    const float2 gains = panGains(v, pan);
+    const float2 gains = panGains(v, s.pan);
     const float l = sample.x * gains.x;
     const float r = sample.y * gains.y;
     if (v.stereoMatrix) {
         float direct = v.widthDirect, cross = v.widthCross;
-        if (widthOffset != 0) {
-            const float width = fminf(1.f, fmaxf(-1.f, v.width + widthOffset));
+        if (s.width != 0) {
+            const float width = fminf(1.f, fmaxf(-1.f, v.width + s.width));
             direct = cosf((1 - width) * kQuarterPi);
             cross = cosf((1 + width) * kQuarterPi);
         }
         float positionLeft = v.positionLeft, positionRight = v.positionRight;
-        if (positionOffset != 0) {
-            const float position = fminf(1.f, fmaxf(-1.f, v.stereoPosition + positionOffset));
+        if (s.position != 0) {
+            const float position = fminf(1.f, fmaxf(-1.f, v.stereoPosition + s.position));
             positionLeft = cosf((1 + position) * kQuarterPi);
             positionRight = cosf((1 - position) * kQuarterPi);
         }
@@ -243,6 +280,26 @@ __device__ __forceinline__ float2 voiceFrame(const float* __restrict__ bank, con
                            fmaf(l, cross, r * direct) * (level * positionRight));
     }
     return make_float2(l * level, r * level);
+}
+
+// Enveloped, modulated, panned voice frame (render.cu:138-187).
+__device__ __forceinline__ float2 voiceFrame(const float* __restrict__ bank, const float* __restrict__ sinc,
+                                             const cs_voice_span& v, const cs_control_point* __restrict__ points,
+                                             const cs_voice_modulation* __restrict__ modulation, float pan,
+                                             int frame, bool filterInput, double phase)
+{
+    const float level = envelopeAt(v, frame);
+    if (level <= 0)
+        return make_float2(0.f, 0.f);
+    VoiceMods s{level, 0.f, pan, 0.f, 0.f};
+    const int modEnd = v.firstModulation + v.modulationCount;
+    for (int j = v.firstModulation; j < modEnd; ++j) {
+        const cs_voice_modulation m = modulation[j];
+        if (m.target > CS_MOD_POSITION)
+            continue;
+        addVoiceMod(s, m.target, bindingAt(m, points, frame));
+    }
+    return voiceOutput(bank, sinc, v, s, frame, filterInput, phase);
 }
 
 // ---- filters (render.cu:276-336) ------------------------------------------------
@@ -362,25 +419,47 @@ __device__ __forceinline__ void filterTargets(const cs_voice_span& v, const cs_c
 
 namespace cs {
 
+// Modulation sums of one of the two main filter slots (render.cu:378-396): cutoff
+// cents, resonance dB and (slot 0) filter-envelope depth, in binding order.
+struct FilterMods {
+    float cents, db, depth;
+};
+
+__device__ __forceinline__ bool filterModTarget(int f, int target)
+{
+    return target == (f == 0 ? CS_MOD_CUTOFF : CS_MOD_CUTOFF2) ||
+        target == (f == 0 ? CS_MOD_RESONANCE : CS_MOD_RESONANCE2) || (f == 0 && target == CS_MOD_FILEG_DEPTH);
+}
+
+__device__ __forceinline__ void addFilterMod(FilterMods& s, int f, int target, float value)
+{
+    if (target == (f == 0 ? CS_MOD_CUTOFF : CS_MOD_CUTOFF2)) s.cents += value;
+    else if (target == (f == 0 ? CS_MOD_RESONANCE : CS_MOD_RESONANCE2)) s.db += value;
+    else if (f == 0 && target == CS_MOD_FILEG_DEPTH) s.depth += value;
+}
+
+// Target coefficients of slot `f` from its modulation sums (render.cu:397-404).
+__device__ __forceinline__ Biquad filterFromMods(const cs_voice_span& v, int f, const FilterMods& s, int frame)
+{
+    float cents = s.cents;
+    if (f == 0 && v.activeEnvelope[0])
+        cents += s.depth * envelopeAt(v.extraEnvelope[0], frame);
+    const cs_voice_filter& filter = v.filters[f];
+    return designFilter(filter.type, filter.cutoff * exp2f(cents / 1200), filter.resonance + s.db, v.sampleRate, 0, 0);
+}
+
 // Target coefficients of one of the two main filter slots at `frame`; the same
 // accumulation as filterTargets restricted to slot `f` (render.cu:378-404).
 __device__ __forceinline__ Biquad filterTargetSlot(const cs_voice_span& v, const cs_control_point* __restrict__ points,
                                                    const cs_voice_modulation* __restrict__ modulation, int frame, int f)
 {
-    float cents = 0, db = 0;
-    float depth = v.extraEnvelope[0].depth;
-    const int cutoffTarget = f == 0 ? CS_MOD_CUTOFF : CS_MOD_CUTOFF2;
-    const int resonanceTarget = f == 0 ? CS_MOD_RESONANCE : CS_MOD_RESONANCE2;
+    FilterMods s{0.f, 0.f, v.extraEnvelope[0].depth};
     for (int j = v.firstModulation; j < v.firstModulation + v.modulationCount; ++j) {
         const cs_voice_modulation m = modulation[j];
-        if (m.target == cutoffTarget) cents += bindingAt(m, points, frame);
-        else if (m.target == resonanceTarget) db += bindingAt(m, points, frame);
-        else if (f == 0 && m.target == CS_MOD_FILEG_DEPTH) depth += bindingAt(m, points, frame);
+        if (filterModTarget(f, m.target))
+            addFilterMod(s, f, m.target, bindingAt(m, points, frame));
     }
-    if (f == 0 && v.activeEnvelope[0])
-        cents += depth * envelopeAt(v.extraEnvelope[0], frame);
-    const cs_voice_filter& filter = v.filters[f];
-    return designFilter(filter.type, filter.cutoff * exp2f(cents / 1200), filter.resonance + db, v.sampleRate, 0, 0);
+    return filterFromMods(v, f, s, frame);
 }
 
 } // namespace cs
