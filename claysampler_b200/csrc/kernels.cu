@@ -323,15 +323,23 @@ __global__ void __launch_bounds__(kSourceTile) sourceKernel(BatchView b, Segment
 
 // ---- TMA-staged serial recurrences --------------------------------------------------
 //
-// Lane = chain.  Each lane keeps two 32-frame chunks of its chain in shared memory,
-// filled by cp.async.bulk copies that complete on the lane's own mbarriers, so the
-// next chunk's sources and targets arrive while the current one runs through the
-// smoothing and biquad recurrence.  Waits are bounded: a wait that runs out sets
-// the batch's error flag and the lane stops.
+// Two lanes per chain (one per channel), 16 chains per warp.  Each chain keeps
+// kRecBuffers chunks of kRecChunk frames in shared memory, filled by
+// cp.async.bulk copies that its leader lane issues and that complete on the chain's
+// own mbarriers, so the next chunk's sources and targets arrive while the current
+// one runs through the smoothing and biquad recurrence.  The kernel's time is the
+// longest chain's, which is bound by the instructions its warp issues per frame;
+// large chunks keep the per-chunk work (wait, cursor advance, copy issue) small
+// beside the per-frame work.  Waits are bounded: a wait that runs out sets the
+// batch's error flag and the lane stops.
 
-constexpr int kRecChunk = 32;
-constexpr int kRecBuffers = 3;
-constexpr int kRecBuffer = kRecChunk * 2 * 4 + kRecChunk * 3 * 4;     // 640 bytes: sources, targets
+#ifndef CS_REC_CHUNK
+#define CS_REC_CHUNK 128
+#endif
+constexpr int kRecChunk = CS_REC_CHUNK;                               // staged frames, a multiple of 32
+static_assert(kRecChunk % kRecChunkFrames == 0, "staged chunks hold whole target plane groups");
+constexpr int kRecBuffers = 2;
+constexpr int kRecBuffer = kRecChunk * 2 * 4 + kRecChunk * 3 * 4;     // sources, then target plane groups
 constexpr int kRecChainBytes = kRecBuffers * kRecBuffer + 16;         // skew: conflict-free LDS.128
 constexpr int kRecChains = 16;                                        // per warp: lane = 2 * chain + channel
 constexpr int kRecWarps = 2;
@@ -378,32 +386,6 @@ __device__ __forceinline__ bool barrierWait(uint64_t* bar, uint32_t parity)
 
 __device__ __forceinline__ uint32_t round16(uint32_t bytes) { return (bytes + 15u) & ~15u; }
 
-struct ChainCursor {
-    int span, pos, stop, start;         // frames, job-local
-};
-
-__device__ __forceinline__ ChainCursor firstCursor(const cs_voice_span* voices, int from, const SegmentView& s)
-{
-    for (int at = from; at >= 0; at = voices[at].nextFilteredSpan) {
-        const cs_voice_span& v = voices[at];
-        if (v.begin >= s.end)
-            break;
-        if (v.end > s.first) {
-            const int start = max(v.begin, s.first);
-            return {at, start, min(v.end, s.end), start};
-        }
-    }
-    return {-1, 0, 0, 0};
-}
-
-__device__ __forceinline__ ChainCursor advanceCursor(const cs_voice_span* voices, ChainCursor c, const SegmentView& s)
-{
-    c.pos += min(kRecChunk, c.stop - c.pos);
-    if (c.pos < c.stop)
-        return c;
-    return firstCursor(voices, voices[c.span].nextFilteredSpan, s);
-}
-
 // One channel of one chain through staged frames [first, count) of a 32-frame
 // chunk.  Sources are interleaved per frame (stereo) and targets are planar, so
 // aligned groups of four frames need one or two 128-bit loads each; Type fixes
@@ -432,29 +414,44 @@ __device__ __forceinline__ void recurChunk(const float* __restrict__ frames, con
         out[stride * i] = frameStep(x, Moving ? targets[i] : 0.f, Moving ? targets[kRecChunkFrames + i] : 0.f,
                                     Moving ? targets[2 * kRecChunkFrames + i] : 0.f);
     }
-    for (; i + 4 <= count; i += 4) {
-        float x[4];
-        if (Stereo) {
-            const float4 a = *reinterpret_cast<const float4*>(frames + 2 * i);
-            const float4 b2 = *reinterpret_cast<const float4*>(frames + 2 * i + 4);
-            x[0] = channel ? a.y : a.x;
-            x[1] = channel ? a.w : a.z;
-            x[2] = channel ? b2.y : b2.x;
-            x[3] = channel ? b2.w : b2.z;
-        } else {
-            const float4 a = *reinterpret_cast<const float4*>(frames + i);
-            x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+    // Groups of kGroup frames: the coefficient smoothing of the whole group runs
+    // first (it does not depend on the audio), then the biquad steps, so the
+    // warp's in-order issue always has independent work between dependent steps.
+    constexpr int kGroup = 8;
+    for (; i + kGroup <= count; i += kGroup) {
+        float x[kGroup];
+        #pragma unroll
+        for (int k = 0; k < kGroup; ++k)
+            x[k] = frames[stride * (i + k) + channel];
+        Biquad q[kGroup];
+        #pragma unroll
+        for (int k = 0; k < kGroup; k += 4) {
+            float4 t0 = make_float4(0, 0, 0, 0), t1 = t0, t2 = t0;
+            if (Moving) {
+                t0 = *reinterpret_cast<const float4*>(targets + i + k);
+                t1 = *reinterpret_cast<const float4*>(targets + kRecChunkFrames + i + k);
+                t2 = *reinterpret_cast<const float4*>(targets + 2 * kRecChunkFrames + i + k);
+            }
+            const float a0[4] = {t0.x, t0.y, t0.z, t0.w}, a1[4] = {t1.x, t1.y, t1.z, t1.w};
+            const float a2[4] = {t2.x, t2.y, t2.z, t2.w};
+            #pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (Moving) {
+                    c.c0 = fmaf(amount, a0[j] - c.c0, c.c0);
+                    c.c1 = fmaf(amount, a1[j] - c.c1, c.c1);
+                    c.c2 = fmaf(amount, a2[j] - c.c2, c.c2);
+                }
+                q[k + j] = expand(Type, c);
+            }
         }
-        float4 t0 = make_float4(0, 0, 0, 0), t1 = t0, t2 = t0;
-        if (Moving) {
-            t0 = *reinterpret_cast<const float4*>(targets + i);
-            t1 = *reinterpret_cast<const float4*>(targets + kRecChunkFrames + i);
-            t2 = *reinterpret_cast<const float4*>(targets + 2 * kRecChunkFrames + i);
+        #pragma unroll
+        for (int k = 0; k < kGroup; ++k) {
+            float y = x[k];
+            #pragma unroll
+            for (int sct = 0; sct < Sections; ++sct)
+                y = biquadStep(y, q[k], z1[sct], z2[sct]);
+            out[stride * (i + k)] = y;
         }
-        out[stride * (i + 0)] = frameStep(x[0], t0.x, t1.x, t2.x);
-        out[stride * (i + 1)] = frameStep(x[1], t0.y, t1.y, t2.y);
-        out[stride * (i + 2)] = frameStep(x[2], t0.z, t1.z, t2.z);
-        out[stride * (i + 3)] = frameStep(x[3], t0.w, t1.w, t2.w);
     }
     for (; i < count; ++i) {
         const float x = frames[stride * i + channel];
@@ -595,14 +592,16 @@ __global__ void __launch_bounds__(kRecThreads, 1) recurrenceKernel(BatchView b, 
         const int count = min(kRecChunk, next.stop - next.pos);
         const int rel = next.pos - next.start;
         const uint32_t srcBytes = round16(uint32_t(count * next.channels) * 4u);
-        const uint32_t tgtBytes = next.moving ? uint32_t(3 * kRecChunkFrames * 4) : 0u;
+        // Only the plane groups the chunk's frames use (the span's last may be partial).
+        const uint32_t tgtBytes = next.moving ? uint32_t((count + kRecChunkFrames - 1) / kRecChunkFrames) *
+            uint32_t(3 * kRecChunkFrames * 4) : 0u;
         unsigned char* buffer = region + slot * kRecBuffer;
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         barrierExpect(&bars[local][slot], srcBytes + tgtBytes);
         bulkLoad(buffer, next.src + size_t(rel) * next.channels, srcBytes, &bars[local][slot]);
         if (tgtBytes)
-            bulkLoad(buffer + kRecChunk * 2 * 4, next.tgt + size_t(rel / kRecChunk) * 3 * kRecChunk, tgtBytes,
-                     &bars[local][slot]);
+            bulkLoad(buffer + kRecChunk * 2 * 4, next.tgt + size_t(rel / kRecChunkFrames) * 3 * kRecChunkFrames,
+                     tgtBytes, &bars[local][slot]);
     };
     uint32_t phases = 0;                 // bit k: parity of buffer k's next completion
     for (int slot = 0; slot < kRecBuffers && next.span >= 0; ++slot) {
@@ -630,7 +629,7 @@ __global__ void __launch_bounds__(kRecThreads, 1) recurrenceKernel(BatchView b, 
             if (!initialized) {
                 // The chain's first frame takes its targets without smoothing.
                 if (moving)
-                    c = {targets[0], targets[kRecChunk], targets[2 * kRecChunk]};
+                    c = {targets[0], targets[kRecChunkFrames], targets[2 * kRecChunkFrames]};
                 else
                     c = {consume.tgt[0], consume.tgt[1], consume.tgt[2]};
                 initialized = true;
@@ -643,12 +642,18 @@ __global__ void __launch_bounds__(kRecThreads, 1) recurrenceKernel(BatchView b, 
                 out[0] = x;
                 first = 1;
             }
-            if (stride == 2)
-                recurDispatch<true>(type, frames, targets, out, first, count, channel, sections, moving,
-                                    consume.amount, c, z1, z2);
-            else
-                recurDispatch<false>(type, frames, targets, out, first, count, channel, sections, moving,
-                                     consume.amount, c, z1, z2);
+            // One target plane group per 32 frames.
+            for (int half = 0; half * kRecChunkFrames < count; ++half) {
+                const int base = half * kRecChunkFrames;
+                const int n = min(kRecChunkFrames, count - base);
+                const float* planes = targets + half * 3 * kRecChunkFrames;
+                if (stride == 2)
+                    recurDispatch<true>(type, frames + 2 * base, planes, out + 2 * base, half ? 0 : first, n, channel,
+                                        sections, moving, consume.amount, c, z1, z2);
+                else
+                    recurDispatch<false>(type, frames + base, planes, out + base, half ? 0 : first, n, channel,
+                                         sections, moving, consume.amount, c, z1, z2);
+            }
         } else {
             initialized = true;
         }
