@@ -1095,6 +1095,20 @@ __global__ void finalizeKernel(BatchView b, FinishView f, const short* input, in
 
 // ---- launchers --------------------------------------------------------------------------
 
+__global__ void expandTilesKernel(const int4* runs, int count, int2* tiles)
+{
+    const int4 run = runs[blockIdx.x];
+    const int n = (run.z - run.y + kSourceTile - 1) / kSourceTile;
+    for (int k = int(threadIdx.x); k < n; k += blockDim.x)
+        tiles[run.w + k] = make_int2(run.x, run.y + k * kSourceTile);
+}
+
+void launchExpandTiles(const int4* runs, int count, int2* tiles, cudaStream_t stream)
+{
+    if (count)
+        expandTilesKernel<<<count, 128, 0, stream>>>(runs, count, tiles);
+}
+
 void launchScan(const BatchView& b, StereoStats* stats, int blocks, cudaStream_t stream)
 {
     if (blocks)

@@ -154,6 +154,9 @@ struct PackView {
 void buildSincTable(float* phaseMajor);   // host: 2049 x 48 floats
 
 void launchScan(const BatchView& b, StereoStats* stats, int blocks, cudaStream_t stream);
+// Source tiles (span, first frame) every kSourceTile frames of each run
+// (span, first frame, end frame, first tile).
+void launchExpandTiles(const int4* runs, int count, int2* tiles, cudaStream_t stream);
 void launchPitch(const BatchView& b, const SegmentView& s, cudaStream_t stream);
 int launchSources(const BatchView& b, const SegmentView& s, cudaStream_t stream);
 int launchRecurrences(const BatchView& b, const SegmentView& s, cudaStream_t stream);

@@ -7,6 +7,7 @@
 // 1024-frame-aligned segments and chain state (filter history, coefficient
 // smoothing, pitch phase) carries across them in ChainState, as the reference's
 // segmented synthesis does (src/cuda/renderer.cpp:864-932, render.cu:228-265,345-446).
+#include "host_copy.hpp"
 #include "kernels.cuh"
 #include "plan_blob.hpp"
 
@@ -195,7 +196,8 @@ struct SegmentTables {
     std::vector<SegmentPlan> segments;
     std::vector<uint64_t> scratchOffset, phaseOffset, targetOffset;   // segments x voices
     std::vector<int> chains, simple, pitch, blocks;
-    std::vector<int2> tiles;
+    std::vector<int4> tileRuns;         // (span, first frame, end frame, first tile) per span
+    size_t tileCount = 0;               // source tiles of all segments
     size_t scratchBytes = 0;
 };
 
@@ -278,20 +280,44 @@ SegmentTables planSegments(const HostBatch& batch, size_t budget)
     };
     const int lastFrame = batch.lastFrame;
     const int blocks = (lastFrame + kBlockFrames - 1) / kBlockFrames;
-    // Per-block storage demand, via spans' block overlaps (slack for alignment).
+    // Per-block storage demand, via spans' block overlaps (slack for alignment): the
+    // partial first and last blocks of a span directly, its full blocks through
+    // difference arrays.
     std::vector<long long> floatsPerBlock(size_t(blocks) + 1, 0), phasesPerBlock(size_t(blocks) + 1, 0);
+    std::vector<long long> fullFloats(size_t(blocks) + 1, 0), fullPhases(size_t(blocks) + 1, 0);
     for (size_t vi = 0; vi < voiceCount; ++vi) {
         const auto& v = batch.voices[vi];
         if (v.filterTrack < 0)
             continue;
-        for (int b = v.begin / kBlockFrames; b <= (v.end - 1) / kBlockFrames; ++b) {
-            const int lo = std::max(v.begin, b * kBlockFrames), hi = std::min(v.end, (b + 1) * kBlockFrames);
-            floatsPerBlock[size_t(b)] += (long long)(hi - lo) * v.channels + 8 +
-                (long long)targetFloats(vi, hi - lo);
+        const auto add = [&](int b, int frames) {
+            floatsPerBlock[size_t(b)] += (long long)frames * v.channels + 8 + (long long)targetFloats(vi, frames);
             if (v.variablePitch)
-                phasesPerBlock[size_t(b)] += hi - lo;
+                phasesPerBlock[size_t(b)] += frames;
+        };
+        const int first = v.begin / kBlockFrames, last = (v.end - 1) / kBlockFrames;
+        if (first == last) {
+            add(first, v.end - v.begin);
+            continue;
+        }
+        add(first, (first + 1) * kBlockFrames - v.begin);
+        add(last, v.end - last * kBlockFrames);
+        if (last - first > 1) {
+            const long long full = (long long)kBlockFrames * v.channels + 8 + (long long)targetFloats(vi, kBlockFrames);
+            fullFloats[size_t(first + 1)] += full;
+            fullFloats[size_t(last)] -= full;
+            if (v.variablePitch) {
+                fullPhases[size_t(first + 1)] += kBlockFrames;
+                fullPhases[size_t(last)] -= kBlockFrames;
+            }
         }
     }
+    for (long long b = 0, floatsRun = 0, phasesRun = 0; b < blocks; ++b) {
+        floatsRun += fullFloats[size_t(b)];
+        phasesRun += fullPhases[size_t(b)];
+        floatsPerBlock[size_t(b)] += floatsRun;
+        phasesPerBlock[size_t(b)] += phasesRun;
+    }
+
     std::vector<std::pair<int, int>> ranges;
     for (int b = 0; b < blocks;) {
         size_t floats = 0, phases = 0;
@@ -352,7 +378,7 @@ SegmentTables planSegments(const HostBatch& batch, size_t budget)
             return false;
         };
         seg.chainFirst = t.chains.size();
-        seg.tileFirst = t.tiles.size();
+        seg.tileFirst = t.tileCount;
         std::vector<std::pair<long long, int>> simpleChains;
         for (int h : batch.chainHeads) {
             if (!active(h))
@@ -366,13 +392,17 @@ SegmentTables planSegments(const HostBatch& batch, size_t budget)
                 const auto& v = batch.voices[size_t(span)];
                 const int lo = std::max(v.begin, seg.first), hi = std::min(v.end, seg.end);
                 frames += std::max(0, hi - lo);
-                for (int f = lo; f < hi; f += kSourceTile)
-                    t.tiles.push_back(make_int2(span, f));
+                if (lo < hi) {
+                    t.tileRuns.push_back(make_int4(span, lo, hi, int(t.tileCount)));
+                    t.tileCount += size_t(hi - lo + kSourceTile - 1) / kSourceTile;
+                }
             }
             simpleChains.emplace_back(-frames, h);
         }
         seg.chainCount = t.chains.size() - seg.chainFirst;
-        seg.tileCount = t.tiles.size() - seg.tileFirst;
+        seg.tileCount = t.tileCount - seg.tileFirst;
+        if (t.tileCount > size_t(INT32_MAX))
+            throw std::runtime_error("too many source tiles in one batch");
         // Longest recurrences first: neighbouring lanes then run similar lengths.
         std::stable_sort(simpleChains.begin(), simpleChains.end(),
                          [](const auto& x, const auto& y) { return x.first < y.first; });
@@ -453,6 +483,16 @@ struct cs_renderer {
     size_t stagingCapacity = 0;
     void* arena = nullptr;              // device arena reused by render_window batches
     size_t arenaCapacity = 0;
+    std::unique_ptr<cs::CopyPool> copier;   // host copies into the staging buffer
+
+    cs::CopyPool& copies()
+    {
+        if (!copier) {
+            const unsigned cores = std::max(1u, std::thread::hardware_concurrency());
+            copier = std::make_unique<cs::CopyPool>(std::min(cores, 16u) - 1);
+        }
+        return *copier;
+    }
 
     // Page-locked host memory that grows on demand (the copy engines read and write
     // it directly).
@@ -537,7 +577,7 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     const size_t oScratchOff = section(t.scratchOffset.size() * sizeof(uint64_t));
     const size_t oPhaseOff = section(t.phaseOffset.size() * sizeof(uint64_t));
     const size_t oTargetOff = section(t.targetOffset.size() * sizeof(uint64_t));
-    const size_t oSourceTiles = section(t.tiles.size() * sizeof(int2));
+    const size_t oTileRuns = section(t.tileRuns.size() * sizeof(int4));
     const size_t oChains = section(t.chains.size() * sizeof(int));
     const size_t oSimple = section(t.simple.size() * sizeof(int));
     const size_t oPitch = section(t.pitch.size() * sizeof(int));
@@ -558,6 +598,7 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     const size_t oWindows = section(size_t(batch.windows) * sizeof(MonoStats));
     const size_t oMono = section(r.natural ? batch.frames * sizeof(short) : 0);
     const size_t oPacked = section(batch.frames * size_t(channels) * sizeof(short));
+    const size_t oSourceTiles = section(t.tileCount * sizeof(int2));
     const size_t oScratch = section(t.scratchBytes);
     const size_t oError = section(sizeof(int));
     p->bodyBytes = size_t(batch.bodyWindows) * sizeof(unsigned long long);
@@ -595,15 +636,16 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     r.record();
     auto* base = static_cast<unsigned char*>(p->arena);
     auto* staging = static_cast<unsigned char*>(cs_renderer::pinned(r.staging, r.stagingCapacity, uploadEnd));
+    std::vector<CopyPiece> pieces;
     const auto stage = [&](size_t offset, const auto& items) {
         if (!items.empty())
-            std::memcpy(staging + offset, items.data(), items.size() * sizeof(items.front()));
+            pieces.push_back({staging + offset, items.data(), items.size() * sizeof(items.front())});
     };
     stage(oVoices, batch.voices);
     {
         unsigned char* at = staging + oPoints;
         for (const auto& [first, count] : batch.pointSources) {
-            std::memcpy(at, first, count * sizeof(cs_control_point));
+            pieces.push_back({at, first, count * sizeof(cs_control_point)});
             at += count * sizeof(cs_control_point);
         }
     }
@@ -616,7 +658,7 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     stage(oScratchOff, t.scratchOffset);
     stage(oPhaseOff, t.phaseOffset);
     stage(oTargetOff, t.targetOffset);
-    stage(oSourceTiles, t.tiles);
+    stage(oTileRuns, t.tileRuns);
     stage(oChains, t.chains);
     stage(oSimple, t.simple);
     stage(oPitch, t.pitch);
@@ -626,7 +668,27 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     stage(oOnsets, batch.onsets);
     stage(oOnsetJob, batch.onsetJob);
     stage(oGroups, p->groups);
-    check(cudaMemcpyAsync(base, staging, uploadEnd, cudaMemcpyHostToDevice, r.stream), "CUDA batch upload");
+    // Copy and upload the staging range in slices: each slice's DMA runs while the
+    // workers copy the next slice.
+    constexpr size_t kSlice = size_t(128) << 20;
+    for (size_t from = 0; from < uploadEnd; from += kSlice) {
+        const size_t to = std::min(uploadEnd, from + kSlice);
+        std::vector<CopyPiece> slice;
+        for (const CopyPiece& piece : pieces) {
+            const size_t a = size_t(static_cast<unsigned char*>(piece.dst) - staging), b = a + piece.bytes;
+            const size_t lo = std::max(a, from), hi = std::min(b, to);
+            if (lo < hi)
+                slice.push_back({staging + lo, static_cast<const unsigned char*>(piece.src) + (lo - a), hi - lo});
+        }
+        r.copies().copy(slice);
+        check(cudaMemcpyAsync(base + from, staging + from, to - from, cudaMemcpyHostToDevice, r.stream),
+              "CUDA batch upload");
+    }
+    // The source tiles (256 frames of one span each) are expanded from the runs on
+    // the device: millions of them for an hour of voices.
+    launchExpandTiles(reinterpret_cast<const int4*>(base + oTileRuns), int(t.tileRuns.size()),
+                      reinterpret_cast<int2*>(base + oSourceTiles), r.stream);
+    check(cudaGetLastError(), "CUDA source tile expansion");
     check(cudaStreamSynchronize(r.stream), "CUDA batch upload");
 
     BatchView& v = p->view;

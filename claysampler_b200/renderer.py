@@ -9,6 +9,8 @@ raises.
 from __future__ import annotations
 
 import ctypes
+import os
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
 from pathlib import Path
 from typing import Callable, Optional
@@ -58,6 +60,30 @@ def library() -> ctypes.CDLL:
         lib.cs_stage_name.restype = c.c_char_p
         _lib = lib
     return _lib
+
+
+_copier: Optional[ThreadPoolExecutor] = None
+
+
+def _copy_out(pointer: int, count: int, dtype) -> np.ndarray:
+    """An owned copy of `count` items at `pointer` (host memory).  Large copies are
+    split over a few threads; numpy releases the GIL while it copies."""
+    global _copier
+    out = np.empty(count, dtype)
+    if not count:
+        return out
+    src = np.ctypeslib.as_array(ctypes.cast(pointer, ctypes.POINTER(np.ctypeslib.as_ctypes_type(dtype))),
+                                shape=(count,))
+    if out.nbytes < (16 << 20):
+        np.copyto(out, src)
+        return out
+    if _copier is None:
+        _copier = ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1))
+    parts = _copier._max_workers
+    bounds = np.linspace(0, count, parts + 1).astype(np.int64)
+    list(_copier.map(lambda i: np.copyto(out[bounds[i]:bounds[i + 1]], src[bounds[i]:bounds[i + 1]]),
+                     range(parts)))
+    return out
 
 
 def _check(status: int) -> None:
@@ -196,8 +222,7 @@ class Renderer:
         def on_publish(_user, batch_ptr, first):
             try:
                 b = batch_ptr.contents
-                pcm = np.ctypeslib.as_array(ctypes.cast(b.pcm, ctypes.POINTER(ctypes.c_int16)),
-                                            shape=(b.pcm_samples,)).copy() if b.pcm_samples else np.zeros(0, np.int16)
+                pcm = _copy_out(b.pcm, b.pcm_samples, np.int16)
                 results = np.frombuffer(ctypes.string_at(b.results, b.result_count * TAIL_RESULT.itemsize),
                                         TAIL_RESULT).copy() if b.result_count else np.zeros(0, TAIL_RESULT)
                 indices = [ctypes.cast(b.job_indices, ctypes.POINTER(ctypes.c_size_t))[i]
