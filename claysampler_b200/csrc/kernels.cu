@@ -281,7 +281,7 @@ __device__ __forceinline__ Biquad expand(int type, const Compact& c)
     }
 }
 
-__global__ void __launch_bounds__(kSourceTile) sourceKernel(BatchView b, SegmentView s)
+__global__ void __launch_bounds__(kSourceTile, 8) sourceKernel(BatchView b, SegmentView s)
 {
     const int2 tile = s.sourceTiles[blockIdx.x];
     const int span = tile.x;
@@ -708,7 +708,7 @@ struct MaxOp { template <class T> __device__ T operator()(T a, T b) const { retu
 struct MinOp { __device__ int operator()(int a, int b) const { return a < b ? a : b; } };
 
 template <bool Natural>
-__global__ void __launch_bounds__(kMixThreads) mixKernel(BatchView b, SegmentView s, StereoStats* stats)
+__global__ void __launch_bounds__(kMixThreads, 8) mixKernel(BatchView b, SegmentView s, StereoStats* stats)
 {
     __shared__ double reduceD[32];
     __shared__ float reduceF[32];
