@@ -134,6 +134,23 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def gather_rows(totals, world):
+    """Every rank's row of per-rank figures (a 1-D tensor on the process group's
+    device), as a (world, fields) array on every rank."""
+    import torch
+    if world == 1:
+        return totals.cpu().numpy()[None]
+    gathered = [torch.zeros_like(totals) for _ in range(world)]
+    torch.distributed.all_gather(gathered, totals)
+    return torch.stack(gathered).cpu().numpy()
+
+
+def combine(rows):
+    """Whole-job figures from per-rank rows (audio-s, device ms per step, e2e s per
+    step, e2e audio-s): audio summed over ranks, times the max over ranks."""
+    return float(rows[:, 0].sum()), float(rows[:, 1].max()), float(rows[:, 2].max()), float(rows[:, 3].sum())
+
+
 def algorithmic_bytes(plans):
     """Bytes each stage must move per launch (source samples read once at the voice's
     step, scratch written/read once, mix written once), from the plans."""
@@ -307,13 +324,7 @@ def run_b200(args):
     e2e_s = sum(e2e_times) / len(e2e_times)
 
     totals = torch.tensor([audio, ms, e2e_s, box.get("audio", 0.0)], dtype=torch.float64, device="cuda")
-    if distributed:
-        gathered = [torch.zeros_like(totals) for _ in range(world)]
-        torch.distributed.all_gather(gathered, totals)
-        rows = torch.stack(gathered).cpu().numpy()
-        total_audio, max_ms, max_e2e, total_e2e_audio = rows[:, 0].sum(), rows[:, 1].max(), rows[:, 2].max(), rows[:, 3].sum()
-    else:
-        total_audio, max_ms, max_e2e, total_e2e_audio = audio, ms, e2e_s, box.get("audio", 0.0)
+    total_audio, max_ms, max_e2e, total_e2e_audio = combine(gather_rows(totals, world))
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
