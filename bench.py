@@ -95,10 +95,16 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.index)],
+                                          "-lms", "50", "-i", str(self.index)],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # nvidia-smi takes a moment to start: wait for its first sample, then keep
+            # only the samples taken from here on (the timed region follows).
+            deadline = time.time() + 5
+            while not self.lines and time.time() < deadline and self.proc.poll() is None:
+                time.sleep(0.01)
+            self.lines.clear()
         except OSError:
             self.proc = None
         return self
