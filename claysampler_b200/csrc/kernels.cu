@@ -344,6 +344,7 @@ constexpr int kRecChainBytes = kRecBuffers * kRecBuffer + 16;         // skew: c
 constexpr int kRecChains = 16;                                        // per warp: lane = 2 * chain + channel
 constexpr int kRecWarps = 2;
 constexpr int kRecThreads = 32 * kRecWarps;
+static_assert(kRecWarps * kRecChains == kRecChainsPerCta, "chains per recurrence CTA");
 constexpr long long kWaitLimit = 1ll << 24;
 
 __device__ __forceinline__ uint32_t sharedAddress(const void* p)

@@ -14,6 +14,7 @@ constexpr int kBlockFrames = CS_TAIL_BLOCK_FRAMES;
 constexpr int kTilesPerBlock = kBlockFrames / kTileFrames;
 constexpr int kSourceTile = 256;         // frames per source-kernel CTA
 constexpr uint64_t kNoTargets = ~uint64_t(0);
+constexpr int kRecChainsPerCta = 32;     // single-slot chains per recurrence CTA
 // Moving-filter targets are stored per 32-frame chunk as three planes
 // (c0[32], c1[32], c2[32]) so the recurrence reads four frames per 128-bit load.
 constexpr int kRecChunkFrames = 32;

@@ -189,6 +189,10 @@ struct SegmentPlan {
     size_t scratchFloats, phaseFrames;
     size_t chainFirst, chainCount, simpleFirst, simpleCount, pitchFirst, pitchCount, blockFirst, blockCount;
     size_t tileFirst, tileCount;
+    // The longest single-slot chains and their source tiles come first: their
+    // recurrences start as soon as their sources are rendered, beside the sources
+    // and recurrences of the rest (0: no split).
+    size_t leadChains, leadTiles;
 };
 
 // Host side of a staged batch: segment boundaries and the per-segment arrays.
@@ -380,6 +384,9 @@ SegmentTables planSegments(const HostBatch& batch, size_t budget)
         seg.chainFirst = t.chains.size();
         seg.tileFirst = t.tileCount;
         std::vector<std::pair<long long, int>> simpleChains;
+        const auto framesIn = [&](const cs_voice_span& v) {
+            return std::max(0, std::min(v.end, seg.end) - std::max(v.begin, seg.first));
+        };
         for (int h : batch.chainHeads) {
             if (!active(h))
                 continue;
@@ -388,24 +395,55 @@ SegmentTables planSegments(const HostBatch& batch, size_t budget)
                 continue;
             }
             long long frames = 0;
-            for (int span = h; span >= 0; span = batch.voices[size_t(span)].nextFilteredSpan) {
-                const auto& v = batch.voices[size_t(span)];
-                const int lo = std::max(v.begin, seg.first), hi = std::min(v.end, seg.end);
-                frames += std::max(0, hi - lo);
-                if (lo < hi) {
-                    t.tileRuns.push_back(make_int4(span, lo, hi, int(t.tileCount)));
-                    t.tileCount += size_t(hi - lo + kSourceTile - 1) / kSourceTile;
-                }
-            }
+            for (int span = h; span >= 0; span = batch.voices[size_t(span)].nextFilteredSpan)
+                frames += framesIn(batch.voices[size_t(span)]);
             simpleChains.emplace_back(-frames, h);
         }
         seg.chainCount = t.chains.size() - seg.chainFirst;
-        seg.tileCount = t.tileCount - seg.tileFirst;
-        if (t.tileCount > size_t(INT32_MAX))
-            throw std::runtime_error("too many source tiles in one batch");
+        const auto simpleChains0 = simpleChains;      // plan order
         // Longest recurrences first: neighbouring lanes then run similar lengths.
         std::stable_sort(simpleChains.begin(), simpleChains.end(),
                          [](const auto& x, const auto& y) { return x.first < y.first; });
+        // Lead chains: those at least half as long as the longest, in whole
+        // recurrence CTAs (measured on the 64-job batch against a quarter and a
+        // third: the rest's recurrences then still fit behind the rest's sources,
+        // and fewer lead CTAs share SMs with the source kernel).
+        size_t lead = 0;
+        if (!simpleChains.empty()) {
+            const long long longest = -simpleChains.front().first;
+            while (lead < simpleChains.size() && -simpleChains[lead].first * 2 >= longest)
+                ++lead;
+            lead = (lead + kRecChainsPerCta - 1) / kRecChainsPerCta * kRecChainsPerCta;
+            if (lead >= simpleChains.size())
+                lead = 0;
+        }
+        seg.leadChains = lead;
+        seg.leadTiles = 0;
+        // Source tiles: the lead chains' first, then the rest, each group in plan
+        // order (neighbouring tiles then read neighbouring samples and tracks).
+        std::vector<char> isLead(voiceCount, 0);
+        for (size_t k = 0; k < lead; ++k)
+            isLead[size_t(simpleChains[k].second)] = 1;
+        for (int group = lead ? 0 : 1; group < 2; ++group) {
+            if (group == 1)
+                seg.leadTiles = lead ? t.tileCount - seg.tileFirst : 0;
+            for (const auto& item : simpleChains0) {
+                const int h = item.second;
+                if ((isLead[size_t(h)] != 0) != (group == 0))
+                    continue;
+                for (int span = h; span >= 0; span = batch.voices[size_t(span)].nextFilteredSpan) {
+                    const auto& v = batch.voices[size_t(span)];
+                    const int lo = std::max(v.begin, seg.first), hi = std::min(v.end, seg.end);
+                    if (lo < hi) {
+                        t.tileRuns.push_back(make_int4(span, lo, hi, int(t.tileCount)));
+                        t.tileCount += size_t(hi - lo + kSourceTile - 1) / kSourceTile;
+                    }
+                }
+            }
+        }
+        seg.tileCount = t.tileCount - seg.tileFirst;
+        if (t.tileCount > size_t(INT32_MAX))
+            throw std::runtime_error("too many source tiles in one batch");
         seg.simpleFirst = t.simple.size();
         for (const auto& item : simpleChains)
             t.simple.push_back(item.second);
@@ -471,6 +509,8 @@ struct cs_renderer {
     cs::TailConfig tail{};
     std::string name;
     cudaStream_t stream = nullptr;
+    cudaStream_t lead = nullptr;        // high-priority stream for the lead chains' recurrences
+    cudaEvent_t leadReady = nullptr, leadDone = nullptr;
     float* sinc = nullptr;
     float* bank = nullptr;
     size_t bankCapacity = 0, uploaded = 0;
@@ -813,9 +853,30 @@ void run(cs_renderer& r, cs_prepared& p, cudaStream_t stream)
         launchPitch(view, s, stream);
         launches += s.pitchCount > 0;
         stage(0);
-        launches += launchSources(view, s, stream);
-        stage(1);
-        launches += launchRecurrences(view, s, stream);
+        if (plan.leadChains) {
+            // Lead chains' sources, then their recurrences on the high-priority
+            // stream beside the rest of the sources and recurrences.
+            SegmentView lead = s, rest = s;
+            lead.sourceTileCount = int(plan.leadTiles);
+            lead.simpleCount = int(plan.leadChains);
+            rest.sourceTiles += plan.leadTiles;
+            rest.sourceTileCount -= int(plan.leadTiles);
+            rest.simple += plan.leadChains;
+            rest.simpleCount -= int(plan.leadChains);
+            launches += launchSources(view, lead, stream);
+            check(cudaEventRecord(r.leadReady, stream), "CUDA event record");
+            check(cudaStreamWaitEvent(r.lead, r.leadReady, 0), "CUDA stream wait");
+            launches += launchRecurrences(view, lead, r.lead);
+            check(cudaEventRecord(r.leadDone, r.lead), "CUDA event record");
+            launches += launchSources(view, rest, stream);
+            stage(1);
+            launches += launchRecurrences(view, rest, stream);
+            check(cudaStreamWaitEvent(stream, r.leadDone, 0), "CUDA stream wait");
+        } else {
+            launches += launchSources(view, s, stream);
+            stage(1);
+            launches += launchRecurrences(view, s, stream);
+        }
         stage(2);
         launches += launchGeneralChains(view, s, stream);
         stage(3);
@@ -1246,6 +1307,11 @@ int cs_renderer_create(int device, int natural, const cs_audio_config* audio, in
             throw std::runtime_error(std::string("claysampler_b200 needs an sm_100 GPU, found ") + prop.name);
         r->name = prop.name;
         cs::check(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking), "CUDA stream");
+        int leastPriority = 0, greatestPriority = 0;
+        cs::check(cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority), "CUDA stream priorities");
+        cs::check(cudaStreamCreateWithPriority(&r->lead, cudaStreamNonBlocking, greatestPriority), "CUDA stream");
+        cs::check(cudaEventCreateWithFlags(&r->leadReady, cudaEventDisableTiming), "CUDA event");
+        cs::check(cudaEventCreateWithFlags(&r->leadDone, cudaEventDisableTiming), "CUDA event");
         std::vector<float> table(size_t(cs::kTaps) * (cs::kPhases + 1));
         cs::buildSincTable(table.data());
         cs::check(cudaMalloc(&r->sinc, table.size() * sizeof(float)), "CUDA sinc table");
@@ -1271,6 +1337,9 @@ void cs_renderer_destroy(cs_renderer* r)
     if (r->hostPcm) cudaFreeHost(r->hostPcm);
     if (r->staging) cudaFreeHost(r->staging);
     if (r->stream) cudaStreamDestroy(r->stream);
+    if (r->lead) cudaStreamDestroy(r->lead);
+    if (r->leadReady) cudaEventDestroy(r->leadReady);
+    if (r->leadDone) cudaEventDestroy(r->leadDone);
     delete r;
 }
 
