@@ -272,6 +272,8 @@ def run_b200(args):
 
     jobs = workload(args, rank)
     plans, bank = plan_jobs(jobs)
+    for plan in plans:                  # inputs in page-locked host memory
+        plan.pin()
     renderer = Renderer(device=local, natural=True, batch_jobs=len(plans))
     renderer.upload_samples(bank)
     prepared = renderer.prepare(plans)

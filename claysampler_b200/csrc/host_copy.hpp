@@ -1,7 +1,7 @@
-// Host-memory copies spread over a few worker threads.  Staging a batch copies its
-// plans' control points (a gigabyte for an hour of LFO-modulated voices) into
-// page-locked memory; one thread moves a few GB/s, so the copy is cut into pieces
-// that the workers and the calling thread take in turn.
+// Host work spread over a few worker threads: copies into the page-locked staging
+// buffer (a gigabyte of control points for an hour of LFO-modulated voices; one
+// thread moves a few GB/s) and the per-job parts of staging a batch.  Work is cut
+// into items that the workers and the calling thread take in turn.
 #pragma once
 
 #include <algorithm>
@@ -9,6 +9,7 @@
 #include <condition_variable>
 #include <cstddef>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -21,15 +22,15 @@ struct CopyPiece {
     size_t bytes;
 };
 
-class CopyPool {
+class WorkerPool {
 public:
-    explicit CopyPool(unsigned workers)
+    explicit WorkerPool(unsigned workers)
     {
         for (unsigned i = 0; i < workers; ++i)
             threads_.emplace_back([this] { work(); });
     }
 
-    ~CopyPool()
+    ~WorkerPool()
     {
         {
             std::lock_guard<std::mutex> lock(mutex_);
@@ -40,8 +41,8 @@ public:
             t.join();
     }
 
-    CopyPool(const CopyPool&) = delete;
-    CopyPool& operator=(const CopyPool&) = delete;
+    WorkerPool(const WorkerPool&) = delete;
+    WorkerPool& operator=(const WorkerPool&) = delete;
 
     // Copies every piece (cut into pieces of at most `grain` bytes) and returns when
     // all are done.
@@ -52,48 +53,58 @@ public:
             for (size_t at = 0; at < p.bytes; at += grain)
                 cut.push_back({static_cast<char*>(p.dst) + at, static_cast<const char*>(p.src) + at,
                                std::min(grain, p.bytes - at)});
-        if (cut.empty())
+        run(cut.size(), [&](size_t i) { std::memcpy(cut[i].dst, cut[i].src, cut[i].bytes); });
+    }
+
+    // Runs task(0) .. task(count - 1) over the workers and the calling thread and
+    // returns when all are done.  Tasks must not throw.
+    void run(size_t count, const std::function<void(size_t)>& task)
+    {
+        if (!count)
             return;
-        if (threads_.empty() || cut.size() == 1) {
-            for (const auto& p : cut)
-                std::memcpy(p.dst, p.src, p.bytes);
+        if (threads_.empty() || count == 1) {
+            for (size_t i = 0; i < count; ++i)
+                task(i);
             return;
         }
         {
             std::lock_guard<std::mutex> lock(mutex_);
-            work_ = &cut;
+            task_ = &task;
+            count_ = count;
             next_.store(0);
             pending_ = threads_.size();
             ++generation_;
         }
         wake_.notify_all();
-        drain(cut);
+        drain(task, count);
         std::unique_lock<std::mutex> lock(mutex_);
         done_.wait(lock, [this] { return pending_ == 0; });
-        work_ = nullptr;
+        task_ = nullptr;
     }
 
 private:
-    void drain(const std::vector<CopyPiece>& cut)
+    void drain(const std::function<void(size_t)>& task, size_t count)
     {
-        for (size_t i = next_.fetch_add(1); i < cut.size(); i = next_.fetch_add(1))
-            std::memcpy(cut[i].dst, cut[i].src, cut[i].bytes);
+        for (size_t i = next_.fetch_add(1); i < count; i = next_.fetch_add(1))
+            task(i);
     }
 
     void work()
     {
         size_t seen = 0;
         for (;;) {
-            const std::vector<CopyPiece>* cut;
+            const std::function<void(size_t)>* task;
+            size_t count;
             {
                 std::unique_lock<std::mutex> lock(mutex_);
                 wake_.wait(lock, [&] { return stop_ || generation_ != seen; });
                 if (stop_)
                     return;
                 seen = generation_;
-                cut = work_;
+                task = task_;
+                count = count_;
             }
-            drain(*cut);
+            drain(*task, count);
             {
                 std::lock_guard<std::mutex> lock(mutex_);
                 if (--pending_ == 0)
@@ -105,7 +116,8 @@ private:
     std::vector<std::thread> threads_;
     std::mutex mutex_;
     std::condition_variable wake_, done_;
-    const std::vector<CopyPiece>* work_ = nullptr;
+    const std::function<void(size_t)>* task_ = nullptr;
+    size_t count_ = 0;
     std::atomic<size_t> next_{0};
     size_t pending_ = 0, generation_ = 0;
     bool stop_ = false;

@@ -73,114 +73,166 @@ struct HostBatch {
     std::vector<uint64_t> volumeGroups;
     int bodyWindows = 0;
 
-    // `assessing`: the quality gate or group volume is on; `quality`: the gate is.
-    void append(const cs_plan& plan, int window, bool natural, bool assessing = false, bool quality = false,
-                const BodyGeometry& body = {1, 1, 1})
+    // Stages `count` plans.  `assessing`: the quality gate or group volume is on;
+    // `quality`: the gate is.  A sequential pass checks the plans and sizes every
+    // job's share of each array; the jobs are then filled in parallel.
+    void build(const cs_plan* plans, size_t count, int window, bool natural, bool assessing, bool quality,
+               const BodyGeometry& body, WorkerPool& pool)
     {
-        if (plan.track_count < 3)
-            throw std::runtime_error("a plan needs its CC7, CC11 and CC10 tracks");
-        const int tileCount = (plan.frames + kTileFrames - 1) / kTileFrames;
-        const int blockCount = (plan.frames + kBlockFrames - 1) / kBlockFrames;
-        const int windowCount = natural ? (plan.frames + window - 1) / window : 0;
-        JobInfo job{};
-        job.offset = frames;
-        job.frames = plan.frames;
-        job.musicEnd = plan.music_end;
-        job.limit = plan.limit;
-        job.fade = plan.fade_frames;
-        job.blockFirst = blocks;
-        job.windowFirst = windows;
-        job.tileFirst = int(tiles.size());
-        std::vector<int> pointOffsets(size_t(plan.track_count) + 1);
-        const int64_t planPoints = plan.track_offsets[plan.track_count] - plan.track_offsets[0];
-        if (pointCount + size_t(planPoints) > size_t(INT32_MAX))
-            throw std::runtime_error("too many control points in one batch");
-        for (int i = 0; i <= plan.track_count; ++i)
-            pointOffsets[size_t(i)] = int(pointCount + size_t(plan.track_offsets[i] - plan.track_offsets[0]));
-        if (planPoints)
-            pointSources.emplace_back(plan.points + plan.track_offsets[0], size_t(planPoints));
-        pointCount += size_t(planPoints);
-        for (int i = 0; i < 4; ++i)
-            job.tracks[i] = pointOffsets[size_t(i)];
-        const int modulationBase = int(modulation.size());
-        for (int m = 0; m < plan.modulation_count; ++m) {
-            cs_voice_modulation binding = plan.modulation[m];
-            if (binding.first >= 0) {
-                binding.last = pointOffsets[size_t(binding.first) + 1];
-                binding.first = pointOffsets[size_t(binding.first)];
-            }
-            if (binding.shapeFirst >= 0) {
-                binding.shapeLast = pointOffsets[size_t(binding.shapeFirst) + 1];
-                binding.shapeFirst = pointOffsets[size_t(binding.shapeFirst)];
-            }
-            modulation.push_back(binding);
-        }
-        // Voice lists per tile via a difference array over tile indices.
-        std::vector<int> counts(size_t(tileCount) + 1, 0);
-        for (int s = 0; s < plan.span_count; ++s) {
-            const auto& span = plan.spans[s];
-            if (span.begin < 0 || span.end > plan.frames || span.begin >= span.end)
-                throw std::runtime_error("span outside its job's frames");
-            ++counts[size_t(span.begin / kTileFrames)];
-            --counts[size_t((span.end - 1) / kTileFrames + 1)];
-        }
-        std::partial_sum(counts.begin(), counts.end(), counts.begin());
-        std::vector<int> cursor(static_cast<size_t>(tileCount), 0);
-        int indexCount = int(indices.size());
-        for (int t = 0; t < tileCount; ++t) {
-            tiles.push_back({indexCount, counts[size_t(t)]});
-            cursor[size_t(t)] = indexCount;
-            indexCount += counts[size_t(t)];
-        }
-        indices.resize(size_t(indexCount));
-        std::vector<int> chainTail(size_t(plan.filter_tracks), -1);
-        for (int s = 0; s < plan.span_count; ++s) {
-            cs_voice_span voice = plan.spans[s];
-            const int index = int(voices.size());
-            for (int t = voice.begin / kTileFrames; t <= (voice.end - 1) / kTileFrames; ++t)
-                indices[size_t(cursor[size_t(t)]++)] = index;
-            voice.firstModulation += modulationBase;
-            if (voice.filterTrack >= 0) {
-                if (voice.filterTrack >= plan.filter_tracks)
+        struct Share {
+            size_t voice, modulation, tile, index, point, onset, block, window, frame;
+            int bodyWindow;
+        };
+        std::vector<Share> at(count + 1);
+        Share next{};
+        for (size_t j = 0; j < count; ++j) {
+            const cs_plan& plan = plans[j];
+            if (plan.track_count < 3)
+                throw std::runtime_error("a plan needs its CC7, CC11 and CC10 tracks");
+            at[j] = next;
+            size_t entries = 0;
+            for (int k = 0; k < plan.span_count; ++k) {
+                const auto& span = plan.spans[k];
+                if (span.begin < 0 || span.end > plan.frames || span.begin >= span.end)
+                    throw std::runtime_error("span outside its job's frames");
+                if (span.filterTrack >= plan.filter_tracks)
                     throw std::runtime_error("span filter track outside the plan's filter_tracks");
-                int& tail = chainTail[size_t(voice.filterTrack)];
-                if (tail < 0) {
-                    chainHeads.push_back(index);
-                    if (voice.variablePitch)
-                        pitchHeads.push_back(index);
-                } else {
-                    voices[size_t(tail)].nextFilteredSpan = index;
-                }
-                tail = index;
-                voice.nextFilteredSpan = -1;
-                for (int i = 0; i < 4; ++i)
-                    voice.filterControls[i] = pointOffsets[size_t(i)];
+                entries += size_t((span.end - 1) / kTileFrames - span.begin / kTileFrames + 1);
             }
-            voices.push_back(voice);
-        }
-        if (assessing) {
-            const int bodyFrames = quality || plan.volume_group ? plan.body_frames : 0;
-            const int onsetCount = quality ? plan.onset_count : 0;
-            assess.push_back({bodyFrames, bodyWindows, int(onsets.size()), onsetCount});
-            for (int i = 0; i < onsetCount; ++i) {
-                if (plan.onsets[i] < 0)
+            const int onsetCount = assessing && quality ? plan.onset_count : 0;
+            for (int k = 0; k < onsetCount; ++k)
+                if (plan.onsets[k] < 0)
                     throw std::runtime_error("negative onset frame");
-                onsets.push_back(plan.onsets[i]);
-                onsetJob.push_back(int(jobs.size()));
-            }
-            bodyWindows += body.windows(bodyFrames);
+            const int64_t points = plan.track_offsets[plan.track_count] - plan.track_offsets[0];
+            next.voice += size_t(plan.span_count);
+            next.modulation += size_t(plan.modulation_count);
+            next.tile += size_t((plan.frames + kTileFrames - 1) / kTileFrames);
+            next.index += entries;
+            next.point += size_t(points);
+            next.onset += size_t(onsetCount);
+            next.block += size_t((plan.frames + kBlockFrames - 1) / kBlockFrames);
+            next.window += natural ? size_t((plan.frames + window - 1) / window) : 0;
+            next.frame += size_t(plan.frames);
+            if (assessing)
+                next.bodyWindow += body.windows(quality || plan.volume_group ? plan.body_frames : 0);
         }
-        volumeGroups.push_back(plan.volume_group);
-        jobBlockFirst.push_back(blocks);
-        for (int b = 0; b < blockCount; ++b)
-            blockJob.push_back(int(jobs.size()));
-        for (int w = 0; w < windowCount; ++w)
-            windowJob.push_back(int(jobs.size()));
-        jobs.push_back(job);
-        frames += size_t(plan.frames);
-        blocks += blockCount;
-        windows += windowCount;
-        lastFrame = std::max(lastFrame, plan.frames);
+        at[count] = next;
+        if (next.point > size_t(INT32_MAX) || next.voice > size_t(INT32_MAX) || next.index > size_t(INT32_MAX) ||
+            next.block > size_t(INT32_MAX) || next.window > size_t(INT32_MAX) || next.tile > size_t(INT32_MAX))
+            throw std::runtime_error("batch too large for 32-bit indices");
+        voices.resize(next.voice);
+        modulation.resize(next.modulation);
+        tiles.resize(next.tile);
+        indices.resize(next.index);
+        blockJob.resize(next.block);
+        windowJob.resize(next.window);
+        jobs.resize(count);
+        jobBlockFirst.resize(count);
+        volumeGroups.resize(count);
+        pointSources.resize(count);
+        if (assessing) {
+            assess.resize(count);
+            onsets.resize(next.onset);
+            onsetJob.resize(next.onset);
+        }
+        std::vector<std::vector<int>> heads(count), pitch(count);
+        pool.run(count, [&](size_t j) {
+            const cs_plan& plan = plans[j];
+            const Share& base = at[j];
+            JobInfo& job = jobs[j];
+            job = JobInfo{};
+            job.offset = base.frame;
+            job.frames = plan.frames;
+            job.musicEnd = plan.music_end;
+            job.limit = plan.limit;
+            job.fade = plan.fade_frames;
+            job.blockFirst = int(base.block);
+            job.windowFirst = int(base.window);
+            job.tileFirst = int(base.tile);
+            // Track offsets rebased onto the batch's point array.
+            std::vector<int> pointOffsets(size_t(plan.track_count) + 1);
+            for (int i = 0; i <= plan.track_count; ++i)
+                pointOffsets[size_t(i)] = int(base.point + size_t(plan.track_offsets[i] - plan.track_offsets[0]));
+            pointSources[j] = {plan.points + plan.track_offsets[0], at[j + 1].point - base.point};
+            for (int i = 0; i < 4; ++i)
+                job.tracks[i] = pointOffsets[size_t(i)];
+            for (int m = 0; m < plan.modulation_count; ++m) {
+                cs_voice_modulation binding = plan.modulation[m];
+                if (binding.first >= 0) {
+                    binding.last = pointOffsets[size_t(binding.first) + 1];
+                    binding.first = pointOffsets[size_t(binding.first)];
+                }
+                if (binding.shapeFirst >= 0) {
+                    binding.shapeLast = pointOffsets[size_t(binding.shapeFirst) + 1];
+                    binding.shapeFirst = pointOffsets[size_t(binding.shapeFirst)];
+                }
+                modulation[base.modulation + size_t(m)] = binding;
+            }
+            // Voice lists per tile via a difference array over tile indices.
+            const int tileCount = (plan.frames + kTileFrames - 1) / kTileFrames;
+            std::vector<int> counts(size_t(tileCount) + 1, 0);
+            for (int k = 0; k < plan.span_count; ++k) {
+                const auto& span = plan.spans[k];
+                ++counts[size_t(span.begin / kTileFrames)];
+                --counts[size_t((span.end - 1) / kTileFrames + 1)];
+            }
+            std::partial_sum(counts.begin(), counts.end(), counts.begin());
+            std::vector<int> cursor(static_cast<size_t>(tileCount), 0);
+            int indexCount = int(base.index);
+            for (int t = 0; t < tileCount; ++t) {
+                tiles[base.tile + size_t(t)] = {indexCount, counts[size_t(t)]};
+                cursor[size_t(t)] = indexCount;
+                indexCount += counts[size_t(t)];
+            }
+            std::vector<int> chainTail(size_t(plan.filter_tracks), -1);
+            for (int k = 0; k < plan.span_count; ++k) {
+                cs_voice_span voice = plan.spans[k];
+                const int index = int(base.voice) + k;
+                for (int t = voice.begin / kTileFrames; t <= (voice.end - 1) / kTileFrames; ++t)
+                    indices[size_t(cursor[size_t(t)]++)] = index;
+                voice.firstModulation += int(base.modulation);
+                if (voice.filterTrack >= 0) {
+                    int& tail = chainTail[size_t(voice.filterTrack)];
+                    if (tail < 0) {
+                        heads[j].push_back(index);
+                        if (voice.variablePitch)
+                            pitch[j].push_back(index);
+                    } else {
+                        voices[size_t(tail)].nextFilteredSpan = index;
+                    }
+                    tail = index;
+                    voice.nextFilteredSpan = -1;
+                    for (int i = 0; i < 4; ++i)
+                        voice.filterControls[i] = pointOffsets[size_t(i)];
+                }
+                voices[size_t(index)] = voice;
+            }
+            if (assessing) {
+                const int bodyFrames = quality || plan.volume_group ? plan.body_frames : 0;
+                const int onsetCount = int(at[j + 1].onset - base.onset);
+                assess[j] = {bodyFrames, base.bodyWindow, int(base.onset), onsetCount};
+                for (int i = 0; i < onsetCount; ++i) {
+                    onsets[base.onset + size_t(i)] = plan.onsets[i];
+                    onsetJob[base.onset + size_t(i)] = int(j);
+                }
+            }
+            volumeGroups[j] = plan.volume_group;
+            jobBlockFirst[j] = int(base.block);
+            for (size_t b = base.block; b < at[j + 1].block; ++b)
+                blockJob[b] = int(j);
+            for (size_t w = base.window; w < at[j + 1].window; ++w)
+                windowJob[w] = int(j);
+        });
+        for (size_t j = 0; j < count; ++j) {
+            chainHeads.insert(chainHeads.end(), heads[j].begin(), heads[j].end());
+            pitchHeads.insert(pitchHeads.end(), pitch[j].begin(), pitch[j].end());
+            lastFrame = std::max(lastFrame, plans[j].frames);
+        }
+        pointCount = next.point;
+        frames = next.frame;
+        blocks = int(next.block);
+        windows = int(next.window);
+        bodyWindows = next.bodyWindow;
     }
 };
 
@@ -523,13 +575,13 @@ struct cs_renderer {
     size_t stagingCapacity = 0;
     void* arena = nullptr;              // device arena reused by render_window batches
     size_t arenaCapacity = 0;
-    std::unique_ptr<cs::CopyPool> copier;   // host copies into the staging buffer
+    std::unique_ptr<cs::WorkerPool> copier;   // host copies into the staging buffer
 
-    cs::CopyPool& copies()
+    cs::WorkerPool& copies()
     {
         if (!copier) {
             const unsigned cores = std::max(1u, std::thread::hardware_concurrency());
-            copier = std::make_unique<cs::CopyPool>(std::min(cores, 16u) - 1);
+            copier = std::make_unique<cs::WorkerPool>(std::min(cores, 16u) - 1);
         }
         return *copier;
     }
@@ -572,6 +624,18 @@ size_t defaultScratchBudget()
     return std::max<size_t>(size_t(1) << 20, std::min(freeBytes / 2, total / 4));
 }
 
+// True for page-locked host memory (cudaHostAlloc'd or registered), which the copy
+// engines read directly.
+bool pageLocked(const void* pointer)
+{
+    cudaPointerAttributes attributes{};
+    if (cudaPointerGetAttributes(&attributes, pointer) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return attributes.type == cudaMemoryTypeHost;
+}
+
 // `shared`: carve the batch from the renderer's reusable arena (render_window
 // batches, one alive at a time) instead of a dedicated allocation.
 cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool shared = false)
@@ -583,8 +647,7 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     HostBatch& batch = p->batch;
     const bool assess = r.audio.enabled || r.groupMinimum > 0;
     const BodyGeometry body = bodyGeometry(r.audio);
-    for (size_t i = 0; i < count; ++i)
-        batch.append(plans[i], r.tail.window, r.natural, assess, r.audio.enabled != 0, body);
+    batch.build(plans, count, r.tail.window, r.natural, assess, r.audio.enabled != 0, body, r.copies());
     p->assess = assess;
     if (assess && r.groupMinimum > 0) {
         // Volume groups: runs of equal nonzero ids (src/cuda/renderer.cpp:1751-1761).
@@ -682,11 +745,20 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
             pieces.push_back({staging + offset, items.data(), items.size() * sizeof(items.front())});
     };
     stage(oVoices, batch.voices);
+    // Control points already in page-locked memory go to the device straight from
+    // the caller's arrays; the rest pass through the staging buffer.
+    std::vector<CopyPiece> direct;
     {
-        unsigned char* at = staging + oPoints;
+        size_t at = oPoints;
         for (const auto& [first, count] : batch.pointSources) {
-            pieces.push_back({at, first, count * sizeof(cs_control_point)});
-            at += count * sizeof(cs_control_point);
+            const size_t bytes = count * sizeof(cs_control_point);
+            if (!bytes)
+                continue;
+            if (pageLocked(first))
+                direct.push_back({base + at, first, bytes});
+            else
+                pieces.push_back({staging + at, first, bytes});
+            at += bytes;
         }
     }
     stage(oMods, batch.modulation);
@@ -708,22 +780,37 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     stage(oOnsets, batch.onsets);
     stage(oOnsetJob, batch.onsetJob);
     stage(oGroups, p->groups);
-    // Copy and upload the staging range in slices: each slice's DMA runs while the
-    // workers copy the next slice.
-    constexpr size_t kSlice = size_t(128) << 20;
-    for (size_t from = 0; from < uploadEnd; from += kSlice) {
-        const size_t to = std::min(uploadEnd, from + kSlice);
-        std::vector<CopyPiece> slice;
-        for (const CopyPiece& piece : pieces) {
-            const size_t a = size_t(static_cast<unsigned char*>(piece.dst) - staging), b = a + piece.bytes;
-            const size_t lo = std::max(a, from), hi = std::min(b, to);
-            if (lo < hi)
-                slice.push_back({staging + lo, static_cast<const unsigned char*>(piece.src) + (lo - a), hi - lo});
-        }
-        r.copies().copy(slice);
-        check(cudaMemcpyAsync(base + from, staging + from, to - from, cudaMemcpyHostToDevice, r.stream),
-              "CUDA batch upload");
+    // Copy and upload the staged ranges in slices: each slice's DMA runs while the
+    // workers copy the next slice.  Ranges are the staged pieces merged across small
+    // gaps (section alignment); the direct uploads follow them in stream order, so
+    // a merged range never leaves stale bytes over a directly uploaded piece.
+    std::vector<std::pair<size_t, size_t>> ranges;
+    for (const CopyPiece& piece : pieces) {
+        const size_t a = size_t(static_cast<unsigned char*>(piece.dst) - staging), b = a + piece.bytes;
+        if (!ranges.empty() && a <= ranges.back().second + 4096)
+            ranges.back().second = std::max(ranges.back().second, b);
+        else
+            ranges.emplace_back(a, b);
     }
+    constexpr size_t kSlice = size_t(128) << 20;
+    for (const auto& [rangeFirst, rangeEnd] : ranges) {
+        for (size_t from = rangeFirst; from < rangeEnd; from += kSlice) {
+            const size_t to = std::min(rangeEnd, from + kSlice);
+            std::vector<CopyPiece> slice;
+            for (const CopyPiece& piece : pieces) {
+                const size_t a = size_t(static_cast<unsigned char*>(piece.dst) - staging), b = a + piece.bytes;
+                const size_t lo = std::max(a, from), hi = std::min(b, to);
+                if (lo < hi)
+                    slice.push_back({staging + lo, static_cast<const unsigned char*>(piece.src) + (lo - a), hi - lo});
+            }
+            r.copies().copy(slice);
+            check(cudaMemcpyAsync(base + from, staging + from, to - from, cudaMemcpyHostToDevice, r.stream),
+                  "CUDA batch upload");
+        }
+    }
+    for (const CopyPiece& piece : direct)
+        check(cudaMemcpyAsync(piece.dst, piece.src, piece.bytes, cudaMemcpyHostToDevice, r.stream),
+              "CUDA batch upload");
     // The source tiles (256 frames of one span each) are expanded from the runs on
     // the device: millions of them for an hour of voices.
     launchExpandTiles(reinterpret_cast<const int4*>(base + oTileRuns), int(t.tileRuns.size()),

@@ -117,6 +117,21 @@ class Plan:
         return b"".join([head, self.spans.tobytes(), self.track_offsets.astype(np.int64).tobytes(),
                          self.points.tobytes(), self.modulation.tobytes(), self.onsets.astype(np.int32).tobytes()])
 
+    def pin(self) -> "Plan":
+        """Moves the plan's arrays into page-locked host memory, from which the
+        renderer's copy engines upload them directly (no staging copy)."""
+        import torch
+        keep = []
+        for name in ("spans", "points", "track_offsets", "modulation", "onsets"):
+            array = np.ascontiguousarray(getattr(self, name))
+            buffer = torch.empty(max(array.nbytes, 1), dtype=torch.uint8, pin_memory=True)
+            pinned = buffer.numpy()[:array.nbytes].view(array.dtype)
+            pinned[...] = array
+            setattr(self, name, pinned)
+            keep.append(buffer)
+        self._pinned = keep
+        return self
+
     @property
     def track_count(self) -> int:
         return len(self.track_offsets) - 1

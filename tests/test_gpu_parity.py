@@ -118,3 +118,24 @@ def test_host_planned_batch_matches_oracle(request, fixture):
     expected_pcm, expected = oracle.finish(expected_mix, plans, True)
     compare_results(results, expected)
     compare_pcm(pcm, expected_pcm)
+
+
+def test_page_locked_plans_render_identically(batch_mini, ref_session):
+    """Control points uploaded straight from page-locked plan arrays give the same
+    render as points passed through the staging buffer."""
+    from claysampler_b200.renderer import Renderer
+    plans = plan_jobs(ref_session, batch_mini)
+    bank = ref_session.bank()
+    outputs = []
+    for pinned in (False, True):
+        if pinned:
+            for plan in plans[::2]:     # a mix of page-locked and pageable plans
+                plan.pin()
+        renderer = Renderer(natural=True)
+        renderer.upload_samples(bank)
+        batches = []
+        renderer.render_window(plans, lambda batch, first: batches.append((first, batch.pcm, batch.results)))
+        renderer.close()
+        outputs.append(batches)
+    (a,), (b,) = outputs
+    assert a[0] == b[0] and np.array_equal(a[1], b[1]) and a[2].tobytes() == b[2].tobytes()
