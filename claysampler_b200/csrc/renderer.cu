@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
 #include <limits>
 #include <memory>
 #include <numeric>
@@ -523,6 +524,7 @@ SegmentTables planSegments(const HostBatch& batch, size_t budget)
 struct cs_prepared {
     cs_renderer* owner = nullptr;
     bool sharedArena = false;
+    int lane = 0;                       // the renderer lane whose streams run the batch
     cs::HostBatch batch;
     cs::SegmentTables tables;
     void* arena = nullptr;
@@ -560,9 +562,17 @@ struct cs_renderer {
     size_t waitingLimit = 0, batchJobs = 64;
     cs::TailConfig tail{};
     std::string name;
-    cudaStream_t stream = nullptr;
-    cudaStream_t lead = nullptr;        // high-priority stream for the lead chains' recurrences
-    cudaEvent_t leadReady = nullptr, leadDone = nullptr;
+    cudaStream_t stream = nullptr;      // lane 0's stream
+    // A lane holds one batch in flight: its stream, a high-priority stream for the
+    // lead chains' recurrences, and the arena its batches reuse.
+    struct Lane {
+        cudaStream_t stream = nullptr, lead = nullptr;
+        cudaEvent_t leadReady = nullptr, leadDone = nullptr;
+        void* arena = nullptr;
+        size_t arenaCapacity = 0;
+    };
+    static constexpr int kLanes = 2;
+    Lane lanes[kLanes];
     float* sinc = nullptr;
     float* bank = nullptr;
     size_t bankCapacity = 0, uploaded = 0;
@@ -573,8 +583,6 @@ struct cs_renderer {
     size_t hostPcmCapacity = 0;
     void* staging = nullptr;            // pinned upload buffer for batch metadata
     size_t stagingCapacity = 0;
-    void* arena = nullptr;              // device arena reused by render_window batches
-    size_t arenaCapacity = 0;
     std::unique_ptr<cs::WorkerPool> copier;   // host copies into the staging buffer
 
     cs::WorkerPool& copies()
@@ -638,11 +646,13 @@ bool pageLocked(const void* pointer)
 
 // `shared`: carve the batch from the renderer's reusable arena (render_window
 // batches, one alive at a time) instead of a dedicated allocation.
-cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool shared = false)
+cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool shared = false, int laneIndex = 0)
 {
     check(cudaSetDevice(r.device), "CUDA device");
     auto p = std::make_unique<cs_prepared>();
     p->owner = &r;
+    p->lane = laneIndex;
+    cs_renderer::Lane& lane = r.lanes[laneIndex];
     p->natural = r.natural;
     HostBatch& batch = p->batch;
     const bool assess = r.audio.enabled || r.groupMinimum > 0;
@@ -711,21 +721,21 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     p->arenaBytes = layout.bytes;
 
     if (shared) {
-        if (p->arenaBytes > r.arenaCapacity) {
-            cudaFree(r.arena);
-            r.live -= r.arenaCapacity;
-            r.arena = nullptr;
-            r.arenaCapacity = 0;
-            cudaError_t status = cudaMalloc(&r.arena, p->arenaBytes);
+        if (p->arenaBytes > lane.arenaCapacity) {
+            cudaFree(lane.arena);
+            r.live -= lane.arenaCapacity;
+            lane.arena = nullptr;
+            lane.arenaCapacity = 0;
+            cudaError_t status = cudaMalloc(&lane.arena, p->arenaBytes);
             if (status != cudaSuccess) {
                 cudaGetLastError();
-                r.arena = nullptr;
+                lane.arena = nullptr;
                 throw CudaError(status, "CUDA batch arena allocation");
             }
-            r.arenaCapacity = p->arenaBytes;
-            r.live += r.arenaCapacity;
+            lane.arenaCapacity = p->arenaBytes;
+            r.live += lane.arenaCapacity;
         }
-        p->arena = r.arena;
+        p->arena = lane.arena;
         p->sharedArena = true;
     } else {
         cudaError_t status = cudaMalloc(&p->arena, p->arenaBytes);
@@ -804,19 +814,19 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
                     slice.push_back({staging + lo, static_cast<const unsigned char*>(piece.src) + (lo - a), hi - lo});
             }
             r.copies().copy(slice);
-            check(cudaMemcpyAsync(base + from, staging + from, to - from, cudaMemcpyHostToDevice, r.stream),
+            check(cudaMemcpyAsync(base + from, staging + from, to - from, cudaMemcpyHostToDevice, lane.stream),
                   "CUDA batch upload");
         }
     }
     for (const CopyPiece& piece : direct)
-        check(cudaMemcpyAsync(piece.dst, piece.src, piece.bytes, cudaMemcpyHostToDevice, r.stream),
+        check(cudaMemcpyAsync(piece.dst, piece.src, piece.bytes, cudaMemcpyHostToDevice, lane.stream),
               "CUDA batch upload");
     // The source tiles (256 frames of one span each) are expanded from the runs on
     // the device: millions of them for an hour of voices.
     launchExpandTiles(reinterpret_cast<const int4*>(base + oTileRuns), int(t.tileRuns.size()),
-                      reinterpret_cast<int2*>(base + oSourceTiles), r.stream);
+                      reinterpret_cast<int2*>(base + oSourceTiles), lane.stream);
     check(cudaGetLastError(), "CUDA source tile expansion");
-    check(cudaStreamSynchronize(r.stream), "CUDA batch upload");
+    check(cudaStreamSynchronize(lane.stream), "CUDA batch upload");
 
     BatchView& v = p->view;
     v.bank = r.bank;
@@ -907,7 +917,7 @@ void run(cs_renderer& r, cs_prepared& p, cudaStream_t stream)
 {
     check(cudaSetDevice(r.device), "CUDA device");
     if (!stream)
-        stream = r.stream;
+        stream = r.lanes[p.lane].stream;
     p.view.bank = r.bank;
     p.view.sinc = r.sinc;
     int launches = 0;
@@ -951,14 +961,15 @@ void run(cs_renderer& r, cs_prepared& p, cudaStream_t stream)
             rest.simple += plan.leadChains;
             rest.simpleCount -= int(plan.leadChains);
             launches += launchSources(view, lead, stream);
-            check(cudaEventRecord(r.leadReady, stream), "CUDA event record");
-            check(cudaStreamWaitEvent(r.lead, r.leadReady, 0), "CUDA stream wait");
-            launches += launchRecurrences(view, lead, r.lead);
-            check(cudaEventRecord(r.leadDone, r.lead), "CUDA event record");
+            const cs_renderer::Lane& lane = r.lanes[p.lane];
+            check(cudaEventRecord(lane.leadReady, stream), "CUDA event record");
+            check(cudaStreamWaitEvent(lane.lead, lane.leadReady, 0), "CUDA stream wait");
+            launches += launchRecurrences(view, lead, lane.lead);
+            check(cudaEventRecord(lane.leadDone, lane.lead), "CUDA event record");
             launches += launchSources(view, rest, stream);
             stage(1);
             launches += launchRecurrences(view, rest, stream);
-            check(cudaStreamWaitEvent(stream, r.leadDone, 0), "CUDA stream wait");
+            check(cudaStreamWaitEvent(stream, lane.leadDone, 0), "CUDA stream wait");
         } else {
             launches += launchSources(view, s, stream);
             stage(1);
@@ -1047,67 +1058,167 @@ public:
     WindowRenderer(cs_renderer& renderer, cs_publish_fn publish, cs_refill_fn refill, void* user)
         : r(renderer), publish(publish), refill(refill), user(user) {}
 
+    ~WindowRenderer()
+    {
+        for (const InFlight& f : flight)       // after an error: unpublished batches
+            cs_prepared_destroy(f.batch);
+    }
+
     void render(const cs_plan* plans, size_t count)
     {
         queue.assign(plans, plans + count);
         size_t first = 0;
         for (;;) {
-            if (first == queue.size()) {
-                const cs_plan* more = nullptr;
-                size_t moreCount = 0;
-                if (!refill || !refill(user, 1, &more, &moreCount) || !moreCount)
+            // Keep up to kLanes batches in flight: the next batch is staged and
+            // launched on a free lane while the others run, and batches are
+            // published in order.
+            while (flight.size() < size_t(cs_renderer::kLanes)) {
+                if (first == queue.size() && !more(flight.empty()))
                     break;
-                checkPlans(more, moreCount);
-                queue.insert(queue.end(), more, more + moreCount);
-            }
-            size_t jobs = batchEnd(first, std::min(queue.size(), first + r.batchJobs)) - first;
-            cs_prepared* prepared = nullptr;
-            for (;;) {
-                try {
-                    prepared = prepare(r, queue.data() + first, jobs, true);
-                    break;
-                } catch (const CudaError& e) {
-                    if (e.code != cudaErrorMemoryAllocation)
-                        throw;
-                    // Allocation recovery: retry with half the jobs, then reject the
-                    // single job (src/cuda/renderer.cpp:947-992).
-                    if (jobs > 1) {
-                        jobs = batchEnd(first, first + jobs / 2) - first;
-                        continue;
-                    }
-                    break;
+                size_t jobs = batchEnd(first, std::min(queue.size(), first + r.batchJobs)) - first;
+                if (splitGroup(first, jobs)) {
+                    // Chunks of a volume group larger than a batch go one at a time.
+                    drain();
+                    first = renderAlone(first, jobs);
+                    continue;
                 }
-            }
-            if (!prepared) {
-                rejectScratch(first);
-                // A split group whose last member was rejected still publishes the
-                // members it retained.
-                const uint64_t id = queue[first].volume_group;
-                if (!chunks.empty() && !(first + 1 < queue.size() && id && queue[first + 1].volume_group == id))
-                    finishGroup(nullptr, first);
-                first += 1;
-                continue;
-            }
-            std::unique_ptr<cs_prepared, void (*)(cs_prepared*)> guard(prepared, cs_prepared_destroy);
-            const uint64_t id = queue[first].volume_group;
-            const bool continues = first + jobs < queue.size() && id && queue[first + jobs].volume_group == id;
-            const bool split = r.groupMinimum > 0 && id && (continues || (first > 0 && queue[first - 1].volume_group == id));
-            if (!split) {
+                const int lane = flight.empty() ? 0 : 1 - flight.front().batch->lane;
+                cs_prepared* prepared = tryPrepare(first, jobs, lane);
+                if (!prepared) {
+                    drain();
+                    first = rejectJob(first);
+                    continue;
+                }
+                if (splitGroup(first, jobs)) {          // a smaller batch now cuts a group
+                    cs_prepared_destroy(prepared);
+                    drain();
+                    first = renderAlone(first, jobs);
+                    continue;
+                }
                 run(r, *prepared, nullptr);
-                publishBatch(*prepared, first);
-            } else {
-                prepared->deferGroups = true;
-                run(r, *prepared, nullptr);
-                if (continues)
-                    retainChunk(*prepared, first);
-                else
-                    finishGroup(prepared, first);
+                flight.push_back({prepared, first});
+                first += jobs;
             }
-            first += jobs;
+            if (flight.empty())
+                break;
+            publishFront();
         }
     }
 
 private:
+    struct InFlight {
+        cs_prepared* batch;
+        size_t first;
+    };
+    std::deque<InFlight> flight;
+
+    // Appends refilled plans (clay::Renderer::Refill); `wait`: block until some are
+    // ready or none remain.
+    bool more(bool wait)
+    {
+        const cs_plan* plans = nullptr;
+        size_t count = 0;
+        if (!refill || !refill(user, wait ? 1 : 0, &plans, &count) || !count)
+            return false;
+        checkPlans(plans, count);
+        queue.insert(queue.end(), plans, plans + count);
+        return true;
+    }
+
+    bool splitGroup(size_t first, size_t jobs) const
+    {
+        const uint64_t id = queue[first].volume_group;
+        const bool continues = first + jobs < queue.size() && id && queue[first + jobs].volume_group == id;
+        return r.groupMinimum > 0 && id && (continues || (first > 0 && queue[first - 1].volume_group == id));
+    }
+
+    void publishFront()
+    {
+        InFlight front = flight.front();
+        flight.pop_front();
+        std::unique_ptr<cs_prepared, void (*)(cs_prepared*)> guard(front.batch, cs_prepared_destroy);
+        publishBatch(*front.batch, front.first);
+    }
+
+    void drain()
+    {
+        while (!flight.empty())
+            publishFront();
+    }
+
+    // Stages `jobs` plans on `lane`; on running out of device memory, first publishes
+    // the batches in flight and releases the other lanes' arenas, then halves the
+    // batch (src/cuda/renderer.cpp:947-992).  Null when a single job does not fit.
+    cs_prepared* tryPrepare(size_t first, size_t& jobs, int lane)
+    {
+        for (;;) {
+            try {
+                return prepare(r, queue.data() + first, jobs, true, lane);
+            } catch (const CudaError& e) {
+                if (e.code != cudaErrorMemoryAllocation)
+                    throw;
+                bool released = false;
+                if (!flight.empty()) {
+                    drain();
+                    released = true;
+                }
+                for (int other = 0; other < cs_renderer::kLanes; ++other) {
+                    cs_renderer::Lane& l = r.lanes[other];
+                    if (other != lane && l.arena) {
+                        check(cudaStreamSynchronize(l.stream), "CUDA lane drain");
+                        cudaFree(l.arena);
+                        r.live -= l.arenaCapacity;
+                        l.arena = nullptr;
+                        l.arenaCapacity = 0;
+                        released = true;
+                    }
+                }
+                if (released)
+                    continue;
+                if (jobs > 1) {
+                    jobs = batchEnd(first, first + jobs / 2) - first;
+                    continue;
+                }
+                return nullptr;
+            }
+        }
+    }
+
+    size_t rejectJob(size_t first)
+    {
+        rejectScratch(first);
+        // A split group whose last member was rejected still publishes the members
+        // it retained.
+        const uint64_t id = queue[first].volume_group;
+        if (!chunks.empty() && !(first + 1 < queue.size() && id && queue[first + 1].volume_group == id))
+            finishGroup(nullptr, first);
+        return first + 1;
+    }
+
+    // One batch with nothing else in flight (chunks of split volume groups), on lane
+    // 0; returns the next job.
+    size_t renderAlone(size_t first, size_t jobs)
+    {
+        cs_prepared* prepared = tryPrepare(first, jobs, 0);
+        if (!prepared)
+            return rejectJob(first);
+        std::unique_ptr<cs_prepared, void (*)(cs_prepared*)> guard(prepared, cs_prepared_destroy);
+        if (!splitGroup(first, jobs)) {
+            run(r, *prepared, nullptr);
+            publishBatch(*prepared, first);
+        } else {
+            const uint64_t id = queue[first].volume_group;
+            const bool continues = first + jobs < queue.size() && queue[first + jobs].volume_group == id;
+            prepared->deferGroups = true;
+            run(r, *prepared, nullptr);
+            if (continues)
+                retainChunk(*prepared, first);
+            else
+                finishGroup(prepared, first);
+        }
+        return first + jobs;
+    }
+
     struct Chunk {
         size_t first = 0;
         std::vector<int> blockJob, jobBlockFirst;
@@ -1393,12 +1504,16 @@ int cs_renderer_create(int device, int natural, const cs_audio_config* audio, in
         if (prop.major < 10)
             throw std::runtime_error(std::string("claysampler_b200 needs an sm_100 GPU, found ") + prop.name);
         r->name = prop.name;
-        cs::check(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking), "CUDA stream");
         int leastPriority = 0, greatestPriority = 0;
         cs::check(cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority), "CUDA stream priorities");
-        cs::check(cudaStreamCreateWithPriority(&r->lead, cudaStreamNonBlocking, greatestPriority), "CUDA stream");
-        cs::check(cudaEventCreateWithFlags(&r->leadReady, cudaEventDisableTiming), "CUDA event");
-        cs::check(cudaEventCreateWithFlags(&r->leadDone, cudaEventDisableTiming), "CUDA event");
+        for (auto& lane : r->lanes) {
+            cs::check(cudaStreamCreateWithFlags(&lane.stream, cudaStreamNonBlocking), "CUDA stream");
+            cs::check(cudaStreamCreateWithPriority(&lane.lead, cudaStreamNonBlocking, greatestPriority),
+                      "CUDA stream");
+            cs::check(cudaEventCreateWithFlags(&lane.leadReady, cudaEventDisableTiming), "CUDA event");
+            cs::check(cudaEventCreateWithFlags(&lane.leadDone, cudaEventDisableTiming), "CUDA event");
+        }
+        r->stream = r->lanes[0].stream;
         std::vector<float> table(size_t(cs::kTaps) * (cs::kPhases + 1));
         cs::buildSincTable(table.data());
         cs::check(cudaMalloc(&r->sinc, table.size() * sizeof(float)), "CUDA sinc table");
@@ -1417,16 +1532,22 @@ void cs_renderer_destroy(cs_renderer* r)
     if (!r)
         return;
     cudaSetDevice(r->device);
-    if (r->stream) cudaStreamSynchronize(r->stream);
+    for (auto& lane : r->lanes)
+        if (lane.stream) cudaStreamSynchronize(lane.stream);
     cudaFree(r->sinc);
     cudaFree(r->bank);
-    cudaFree(r->arena);
+    for (auto& lane : r->lanes) {
+        if (lane.lead) cudaStreamSynchronize(lane.lead);
+        cudaFree(lane.arena);
+    }
     if (r->hostPcm) cudaFreeHost(r->hostPcm);
     if (r->staging) cudaFreeHost(r->staging);
-    if (r->stream) cudaStreamDestroy(r->stream);
-    if (r->lead) cudaStreamDestroy(r->lead);
-    if (r->leadReady) cudaEventDestroy(r->leadReady);
-    if (r->leadDone) cudaEventDestroy(r->leadDone);
+    for (auto& lane : r->lanes) {
+        if (lane.stream) cudaStreamDestroy(lane.stream);
+        if (lane.lead) cudaStreamDestroy(lane.lead);
+        if (lane.leadReady) cudaEventDestroy(lane.leadReady);
+        if (lane.leadDone) cudaEventDestroy(lane.leadDone);
+    }
     delete r;
 }
 
