@@ -708,50 +708,107 @@ struct SumOp { template <class T> __device__ T operator()(T a, T b) const { retu
 struct MaxOp { template <class T> __device__ T operator()(T a, T b) const { return a > b ? a : b; } };
 struct MinOp { __device__ int operator()(int a, int b) const { return a < b ? a : b; } };
 
-template <bool Natural>
-__global__ void __launch_bounds__(kMixThreads, 8) mixKernel(BatchView b, SegmentView s, StereoStats* stats)
+// A tile's voice as the mix reads it: frame range, where its filtered frames
+// start (in floats, relative to frame 0 of the job), its index and kind.
+struct MixVoice {
+    long long offset;                   // filtered + offset + frame * channels is the frame's first sample
+    int begin, end, index, kind;        // kind: 0 unfiltered, 1 filtered stereo, 2 filtered mono
+};
+
+constexpr int kMixStaged = kMixThreads / kTilesPerBlock;     // staged voices per tile
+
+// Inline: the batch has unfiltered voices, which the mix renders itself (the
+// general kernel, given more registers for the resampler); without them a lighter
+// kernel keeps 64 warps resident.
+template <bool Natural, bool Inline>
+__global__ void __launch_bounds__(kMixThreads, Inline ? 5 : 8) mixKernel(BatchView b, SegmentView s, StereoStats* stats)
 {
     __shared__ double reduceD[32];
     __shared__ float reduceF[32];
+    // The four tiles' voice lists, staged once for the block's 1024 frames, so a
+    // frame's walk over its voices reads shared memory and then the voice's samples.
+    __shared__ MixVoice staged[kTilesPerBlock][kMixStaged];
+    __shared__ MixTile tiles[kTilesPerBlock];
     const int block = s.blocks[blockIdx.x];
     const int jobIndex = b.blockJob[block];
     const JobInfo job = b.jobs[jobIndex];
     const int local = block - job.blockFirst;
+    const int jobTiles = (job.frames + kTileFrames - 1) / kTileFrames;
+    {
+        const int k = int(threadIdx.x) / kMixStaged, i = int(threadIdx.x) % kMixStaged;
+        const int tileIndex = local * kTilesPerBlock + k;
+        const MixTile tile = tileIndex < jobTiles ? b.tiles[job.tileFirst + tileIndex] : MixTile{0, 0};
+        if (i == 0)
+            tiles[k] = tile;
+        if (i < tile.count && tile.count <= kMixStaged) {
+            const int index = __ldg(b.indices + tile.first + i);
+            const cs_voice_span& v = b.voices[index];
+            MixVoice m;
+            m.begin = v.begin;
+            m.end = v.end;
+            m.index = index;
+            if (v.filterTrack >= 0) {
+                m.kind = v.channels == 1 ? 2 : 1;
+                m.offset = (long long)s.scratchOffset[index] - (long long)max(v.begin, s.first) * v.channels;
+            } else {
+                m.kind = 0;
+                m.offset = 0;
+            }
+            staged[k][i] = m;
+        }
+    }
+    __syncthreads();
     double power = 0;
     float peak = 0;
     for (int k = 0; k < kTilesPerBlock; ++k) {
         const int frame = local * kBlockFrames + k * kTileFrames + int(threadIdx.x);
         if (frame >= job.frames || frame < s.first || frame >= s.end)
             continue;
-        const MixTile tile = b.tiles[job.tileFirst + local * kTilesPerBlock + k];
+        const MixTile tile = tiles[k];
         const float pan = trackAt(b.points, job.tracks[2], job.tracks[3], frame);
         float left = 0, right = 0, wetLeft = 0, wetRight = 0;
-        for (int i = tile.first; i < tile.first + tile.count; ++i) {
-            const int index = __ldg(b.indices + i);
-            const cs_voice_span& v = b.voices[index];
-            if (frame < v.begin || frame >= v.end)
-                continue;
-            if (v.filterTrack >= 0) {
-                const float* src = b.filtered + s.scratchOffset[index] + size_t(frame - max(v.begin, s.first)) *
-                    v.channels;
-                float2 sample = make_float2(src[0], v.channels == 1 ? src[0] : src[1]);
-                if (v.channels == 1) {
-                    float offset = pan;
-                    for (int j = v.firstModulation; j < v.firstModulation + v.modulationCount; ++j) {
-                        const cs_voice_modulation m = b.modulation[j];
-                        if (m.target == CS_MOD_PAN)
-                            offset += bindingAt(m, b.points, frame);
-                    }
-                    const float2 gains = panGains(v, offset);
-                    sample.x *= gains.x;
-                    sample.y *= gains.y;
-                }
+        const auto addVoice = [&](const MixVoice& m) {
+            if (frame < m.begin || frame >= m.end)
+                return;
+            if (m.kind == 1) {
+                const float2 sample = *reinterpret_cast<const float2*>(b.filtered + (m.offset + 2ll * frame));
                 wetLeft += sample.x;
                 wetRight += sample.y;
-            } else {
-                const float2 sample = voiceFrame(b.bank, b.sinc, v, b.points, b.modulation, pan, frame, false, -1.0);
+            } else if (m.kind == 2) {
+                // Mono filtered voices are panned after the filter.
+                const cs_voice_span& v = b.voices[m.index];
+                const float x = b.filtered[m.offset + frame];
+                float offset = pan;
+                for (int j = v.firstModulation; j < v.firstModulation + v.modulationCount; ++j) {
+                    const cs_voice_modulation mod = b.modulation[j];
+                    if (mod.target == CS_MOD_PAN)
+                        offset += bindingAt(mod, b.points, frame);
+                }
+                const float2 gains = panGains(v, offset);
+                wetLeft += x * gains.x;
+                wetRight += x * gains.y;
+            } else if (Inline) {
+                const float2 sample = voiceFrame(b.bank, b.sinc, b.voices[m.index], b.points, b.modulation, pan,
+                                                 frame, false, -1.0);
                 left += sample.x;
                 right += sample.y;
+            }
+        };
+        if (tile.count <= kMixStaged) {
+            for (int i = 0; i < tile.count; ++i)
+                addVoice(staged[k][i]);
+        } else {
+            for (int i = tile.first; i < tile.first + tile.count; ++i) {
+                const int index = __ldg(b.indices + i);
+                const cs_voice_span& v = b.voices[index];
+                MixVoice m;
+                m.begin = v.begin;
+                m.end = v.end;
+                m.index = index;
+                m.kind = v.filterTrack < 0 ? 0 : v.channels == 1 ? 2 : 1;
+                m.offset = v.filterTrack < 0 ? 0
+                    : (long long)s.scratchOffset[index] - (long long)max(v.begin, s.first) * v.channels;
+                addVoice(m);
             }
         }
         const float amplitude = jobGainAt(b.points, job.tracks, frame);
@@ -1159,10 +1216,17 @@ void launchMix(const BatchView& b, const SegmentView& s, bool natural, StereoSta
 {
     if (!s.blockCount)
         return;
-    if (natural)
-        mixKernel<true><<<s.blockCount, kMixThreads, 0, stream>>>(b, s, stats);
-    else
-        mixKernel<false><<<s.blockCount, kMixThreads, 0, stream>>>(b, s, stats);
+    if (natural) {
+        if (b.inlineVoices)
+            mixKernel<true, true><<<s.blockCount, kMixThreads, 0, stream>>>(b, s, stats);
+        else
+            mixKernel<true, false><<<s.blockCount, kMixThreads, 0, stream>>>(b, s, stats);
+    } else {
+        if (b.inlineVoices)
+            mixKernel<false, true><<<s.blockCount, kMixThreads, 0, stream>>>(b, s, stats);
+        else
+            mixKernel<false, false><<<s.blockCount, kMixThreads, 0, stream>>>(b, s, stats);
+    }
 }
 
 int launchFinish(const BatchView& b, const FinishView& f, bool natural, bool quality, const TailConfig& tail,

@@ -69,6 +69,7 @@ struct BatchView {
     void* mix;                          // float2 (natural) or short2
     int* error;                         // set by kernels whose bounded waits ran out
     int jobCount;
+    int inlineVoices;                   // some voice has no filter chain (the mix renders it)
 };
 
 struct SegmentView {

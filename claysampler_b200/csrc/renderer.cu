@@ -844,6 +844,8 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     v.mix = base + oMix;
     v.error = reinterpret_cast<int*>(base + oError);
     v.jobCount = int(jobs);
+    v.inlineVoices = std::any_of(batch.voices.begin(), batch.voices.end(),
+                                 [](const cs_voice_span& voice) { return voice.filterTrack < 0; }) ? 1 : 0;
     const size_t voiceCount = batch.voices.size();
     for (const auto& seg : t.segments) {
         SegmentView s{};
