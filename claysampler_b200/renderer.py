@@ -209,11 +209,13 @@ class Renderer:
         return Prepared(self, plans)
 
     def render_window(self, plans: list[Plan], publish: Callable[[RenderBatch, int], None],
-                      refill: Optional[Callable[[bool], list[Plan]]] = None) -> None:
+                      refill: Optional[Callable[[bool], list[Plan]]] = None, copy: bool = True) -> None:
         """Render every plan; ``publish(batch, first)`` receives each finished batch.
 
         ``refill(wait)`` may return more plans (or an empty list when none are ready),
-        like the reference's Refill callback.
+        like the reference's Refill callback.  With ``copy=False`` the batch's PCM is
+        a view of the renderer's page-locked download buffer, valid only until
+        ``publish`` returns (copy what must outlive the call), as in the C ABI.
         """
         array = c_plans(plans)
         keep = [array]
@@ -222,7 +224,13 @@ class Renderer:
         def on_publish(_user, batch_ptr, first):
             try:
                 b = batch_ptr.contents
-                pcm = _copy_out(b.pcm, b.pcm_samples, np.int16)
+                if copy:
+                    pcm = _copy_out(b.pcm, b.pcm_samples, np.int16)
+                elif b.pcm_samples:
+                    pcm = np.ctypeslib.as_array(ctypes.cast(b.pcm, ctypes.POINTER(ctypes.c_int16)),
+                                                shape=(b.pcm_samples,))
+                else:
+                    pcm = np.zeros(0, np.int16)
                 results = np.frombuffer(ctypes.string_at(b.results, b.result_count * TAIL_RESULT.itemsize),
                                         TAIL_RESULT).copy() if b.result_count else np.zeros(0, TAIL_RESULT)
                 indices = [ctypes.cast(b.job_indices, ctypes.POINTER(ctypes.c_size_t))[i]

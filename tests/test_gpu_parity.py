@@ -139,3 +139,17 @@ def test_page_locked_plans_render_identically(batch_mini, ref_session):
         outputs.append(batches)
     (a,), (b,) = outputs
     assert a[0] == b[0] and np.array_equal(a[1], b[1]) and a[2].tobytes() == b[2].tobytes()
+
+
+def test_zero_copy_publish_matches_copied(plain_small, ref_session):
+    """render_window(copy=False) hands publish a view of the download buffer; read
+    during the callback it holds the same PCM as the copying default."""
+    from claysampler_b200.renderer import Renderer
+    plans = plan_jobs(ref_session, plain_small)
+    renderer = Renderer(natural=True)
+    renderer.upload_samples(ref_session.bank())
+    copied, viewed = [], []
+    renderer.render_window(plans, lambda batch, first: copied.append(batch.pcm))
+    renderer.render_window(plans, lambda batch, first: viewed.append(batch.pcm.copy()), copy=False)
+    renderer.close()
+    assert len(copied) == len(viewed) == 1 and np.array_equal(copied[0], viewed[0])
