@@ -521,6 +521,12 @@ SegmentTables planSegments(const HostBatch& batch, size_t budget)
 } // namespace
 } // namespace cs
 
+namespace cs {
+namespace {
+class WindowRenderer;
+}
+}
+
 struct cs_prepared {
     cs_renderer* owner = nullptr;
     bool sharedArena = false;
@@ -584,6 +590,8 @@ struct cs_renderer {
     void* staging = nullptr;            // pinned upload buffer for batch metadata
     size_t stagingCapacity = 0;
     std::unique_ptr<cs::WorkerPool> copier;   // host copies into the staging buffer
+    // The job queue and batches in flight behind cs_submit / cs_poll.
+    std::unique_ptr<cs::WindowRenderer> service;
 
     cs::WorkerPool& copies()
     {
@@ -1069,41 +1077,92 @@ public:
     void render(const cs_plan* plans, size_t count)
     {
         queue.assign(plans, plans + count);
-        size_t first = 0;
+        next = 0;
         for (;;) {
-            // Keep up to kLanes batches in flight: the next batch is staged and
-            // launched on a free lane while the others run, and batches are
-            // published in order.
-            while (flight.size() < size_t(cs_renderer::kLanes)) {
-                if (first == queue.size() && !more(flight.empty()))
-                    break;
-                size_t jobs = batchEnd(first, std::min(queue.size(), first + r.batchJobs)) - first;
-                if (splitGroup(first, jobs)) {
-                    // Chunks of a volume group larger than a batch go one at a time.
-                    drain();
-                    first = renderAlone(first, jobs);
-                    continue;
-                }
-                const int lane = flight.empty() ? 0 : 1 - flight.front().batch->lane;
-                cs_prepared* prepared = tryPrepare(first, jobs, lane);
-                if (!prepared) {
-                    drain();
-                    first = rejectJob(first);
-                    continue;
-                }
-                if (splitGroup(first, jobs)) {          // a smaller batch now cuts a group
-                    cs_prepared_destroy(prepared);
-                    drain();
-                    first = renderAlone(first, jobs);
-                    continue;
-                }
-                run(r, *prepared, nullptr);
-                flight.push_back({prepared, first});
-                first += jobs;
-            }
+            launch(true);
             if (flight.empty())
                 break;
             publishFront();
+        }
+    }
+
+    // cs_submit: queues plans and launches what the free lanes take; returns the
+    // ticket (queue position) of the first plan.
+    size_t submit(const cs_plan* plans, size_t count)
+    {
+        const size_t ticket = queue.size();
+        queue.insert(queue.end(), plans, plans + count);
+        launch(false);
+        return ticket;
+    }
+
+    // cs_poll: publishes the oldest batch in flight once it is done (waiting for it
+    // when `wait`), then launches queued plans into the lanes that freed up.
+    // Returns the jobs published.
+    size_t poll(bool wait, cs_publish_fn fn, void* data)
+    {
+        publish = fn;
+        user = data;
+        size_t published = 0;
+        while (!flight.empty()) {
+            const cudaError_t state = cudaEventQuery(flight.front().batch->end);
+            if (state != cudaSuccess && state != cudaErrorNotReady)
+                check(state, "CUDA batch completion");
+            if (state == cudaErrorNotReady && !wait)
+                break;
+            published += flight.front().batch->batch.jobs.size();
+            publishFront();
+            launch(false);
+            wait = false;                       // one blocking wait per call at most
+        }
+        launch(false);
+        return published;
+    }
+
+    size_t pending() const { return queue.size() - next; }
+    size_t inFlight() const { return flight.size(); }
+    size_t inFlightJobs() const
+    {
+        size_t jobs = 0;
+        for (const InFlight& f : flight)
+            jobs += f.batch->batch.jobs.size();
+        return jobs;
+    }
+
+private:
+    size_t next = 0;                            // first queued plan not yet launched
+
+    // Keeps up to kLanes batches in flight: the next batch is staged and launched
+    // on a free lane while the others run (batches are published in order).
+    // `mayRefill`: ask the refill callback for more plans when the queue runs dry.
+    void launch(bool mayRefill)
+    {
+        while (flight.size() < size_t(cs_renderer::kLanes)) {
+            if (next == queue.size() && !(mayRefill && more(flight.empty())))
+                break;
+            size_t jobs = batchEnd(next, std::min(queue.size(), next + r.batchJobs)) - next;
+            if (splitGroup(next, jobs)) {
+                // Chunks of a volume group larger than a batch go one at a time.
+                drain();
+                next = renderAlone(next, jobs);
+                continue;
+            }
+            const int lane = flight.empty() ? 0 : 1 - flight.front().batch->lane;
+            cs_prepared* prepared = tryPrepare(next, jobs, lane);
+            if (!prepared) {
+                drain();
+                next = rejectJob(next);
+                continue;
+            }
+            if (splitGroup(next, jobs)) {              // a smaller batch now cuts a group
+                cs_prepared_destroy(prepared);
+                drain();
+                next = renderAlone(next, jobs);
+                continue;
+            }
+            run(r, *prepared, nullptr);
+            flight.push_back({prepared, next});
+            next += jobs;
         }
     }
 
@@ -1533,6 +1592,7 @@ void cs_renderer_destroy(cs_renderer* r)
 {
     if (!r)
         return;
+    r->service.reset();
     cudaSetDevice(r->device);
     for (auto& lane : r->lanes)
         if (lane.stream) cudaStreamSynchronize(lane.stream);
@@ -1697,8 +1757,43 @@ int cs_render_window(cs_renderer* r, const cs_plan* plans, size_t count, cs_publ
         if (!r || !publish)
             throw std::runtime_error("null renderer or publish callback");
         cs::checkPlans(plans, count);
+        if (r->service && (r->service->pending() || r->service->inFlight()))
+            throw std::runtime_error("submitted jobs are still being rendered: poll them first");
         cs::WindowRenderer(*r, publish, refill, user).render(plans, count);
     });
+}
+
+int cs_submit(cs_renderer* r, const cs_plan* plans, size_t count, uint64_t* first_ticket)
+{
+    return cs::guarded([&] {
+        if (!r)
+            throw std::runtime_error("null renderer");
+        cs::checkPlans(plans, count);
+        if (!r->service)
+            r->service = std::make_unique<cs::WindowRenderer>(*r, nullptr, nullptr, nullptr);
+        const size_t ticket = r->service->submit(plans, count);
+        if (first_ticket)
+            *first_ticket = ticket;
+    });
+}
+
+int cs_poll(cs_renderer* r, int wait, cs_publish_fn publish, void* user, size_t* published)
+{
+    return cs::guarded([&] {
+        if (!r || !publish)
+            throw std::runtime_error("null renderer or publish callback");
+        const size_t count = r->service ? r->service->poll(wait != 0, publish, user) : 0;
+        if (published)
+            *published = count;
+    });
+}
+
+size_t cs_pending_jobs(const cs_renderer* r)
+{
+    if (!r || !r->service)
+        return 0;
+    size_t jobs = r->service->pending();
+    return jobs + r->service->inFlightJobs();
 }
 
 const char* cs_renderer_device(const cs_renderer* r) { return r ? r->name.c_str() : ""; }

@@ -55,6 +55,10 @@ def library() -> ctypes.CDLL:
         lib.cs_prepared_segments.restype = sz
         lib.cs_prepared_destroy.argtypes = [vp]
         lib.cs_renderer_set_scratch_limit.argtypes = [vp, sz]
+        lib.cs_submit.argtypes = [vp, vp, sz, c.POINTER(c.c_uint64)]
+        lib.cs_poll.argtypes = [vp, i32, vp, vp, c.POINTER(sz)]
+        lib.cs_pending_jobs.argtypes = [vp]
+        lib.cs_pending_jobs.restype = sz
         lib.cs_prepared_set_profile.argtypes = [vp, i32]
         lib.cs_prepared_stage_ms.argtypes = [vp, vp, i32]
         lib.cs_stage_name.restype = c.c_char_p
@@ -257,6 +261,53 @@ class Renderer:
         if errors:
             raise errors[0]
         _check(status)
+
+    # ---- serving: non-blocking submission (continuous batching) -------------------
+
+    def submit(self, plans: list[Plan]) -> int:
+        """Queues plans for rendering and returns at once (after launching what the
+        free stream lanes take); returns the ticket of the first plan.  Tickets
+        number submitted plans in order."""
+        array = c_plans(plans)
+        ticket = ctypes.c_uint64()
+        _check(library().cs_submit(self.handle, array, len(plans), ctypes.byref(ticket)))
+        if not hasattr(self, "_submitted"):
+            self._submitted = {}
+        self._submitted[ticket.value] = (ticket.value + len(plans), array, plans)
+        return ticket.value
+
+    def poll(self, publish: Callable[[RenderBatch, int], None], wait: bool = False) -> int:
+        """Publishes finished batches in order (``publish(batch, first_ticket)``),
+        waiting for the oldest one when ``wait``, and admits queued plans into the
+        freed lanes; returns the jobs published."""
+        errors = []
+
+        def on_publish(_user, batch_ptr, first):
+            try:
+                b = batch_ptr.contents
+                pcm = _copy_out(b.pcm, b.pcm_samples, np.int16)
+                results = np.frombuffer(ctypes.string_at(b.results, b.result_count * TAIL_RESULT.itemsize),
+                                        TAIL_RESULT).copy() if b.result_count else np.zeros(0, TAIL_RESULT)
+                publish(RenderBatch(pcm, results, b.kernel_seconds, b.failed_scratch_bytes, []), first)
+            except Exception as exc:
+                errors.append(exc)
+
+        callback = PUBLISH(on_publish)
+        count = ctypes.c_size_t()
+        status = library().cs_poll(self.handle, int(wait), ctypes.cast(callback, ctypes.c_void_p), None,
+                                   ctypes.byref(count))
+        if errors:
+            raise errors[0]
+        _check(status)
+        # Release the arrays of submissions whose jobs have all been published.
+        done = self.pending_jobs == 0
+        for key in [k for k, v in getattr(self, "_submitted", {}).items() if done]:
+            del self._submitted[key]
+        return count.value
+
+    @property
+    def pending_jobs(self) -> int:
+        return library().cs_pending_jobs(self.handle)
 
     @property
     def device(self) -> str:

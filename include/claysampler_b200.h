@@ -191,6 +191,21 @@ int cs_upload_samples(cs_renderer* renderer, const float* pcm, size_t floats, in
 int cs_render_window(cs_renderer* renderer, const cs_plan* plans, size_t count,
                      cs_publish_fn publish, cs_refill_fn refill, void* user);
 
+/* ---- serving: non-blocking submission (no reference counterpart) ---------------
+ * Continuous batching for a render service: cs_submit queues plans and returns at
+ * once, after staging and launching what the renderer's free stream lanes take
+ * (two batches in flight, each up to batch_jobs plans; volume-group rules as in
+ * cs_render_window).  cs_poll publishes finished batches in order through
+ * `publish` (whose `first` is the ticket of the batch's first job) and admits queued
+ * plans into the lanes that freed up; with `wait` it blocks for the oldest batch
+ * in flight.  Tickets number submitted plans from 0 in submission order.  A
+ * plan's arrays must stay valid until its job is published.  cs_render_window
+ * refuses to run while submitted jobs are unpublished. */
+int cs_submit(cs_renderer* renderer, const cs_plan* plans, size_t count, uint64_t* first_ticket);
+int cs_poll(cs_renderer* renderer, int wait, cs_publish_fn publish, void* user, size_t* published);
+/* Submitted jobs not yet published (queued or in flight). */
+size_t cs_pending_jobs(const cs_renderer* renderer);
+
 /* Getters (src/cuda/renderer.h:54-59). */
 const char* cs_renderer_device(const cs_renderer* renderer);
 size_t cs_peak_bytes(const cs_renderer* renderer);
