@@ -12,8 +12,12 @@ natural-tail finishing to packed mono PCM16.  `value` times steps on inputs that
 are already resident in device memory (bank 497 MB and per-step scratch well
 above the 126 MB L2, so no flush is needed); `e2e` times the public
 render_window call with the plans in host memory, including the plan upload and
-the PCM download.  Under torchrun every rank renders its own batch (no
-collective), so scaling is weak.
+the PCM download (GPU batches of 32 jobs, the CLI's --gpu-batch-jobs, so that two
+batches in flight overlap their transfers with each other's kernels).  Under
+torchrun every rank renders its own batch (no collective), so scaling is weak.
+
+`--serve` measures instead the submit-to-publish latency of requests that arrive
+one at a time (Poisson) through the non-blocking submit / poll pair.
 
 `--impl reference` times the reference's own CPU implementation of the path
 (its src/cuda/render.cu built for the host, see oracle/ref) on a bounded sample
@@ -52,6 +56,13 @@ def parse():
     p.add_argument("--seed", type=int, default=2)
     p.add_argument("--cpu-sample-jobs", type=int, default=32)
     p.add_argument("--workdir", type=Path, default=Path(tempfile.gettempdir()) / "claysampler_bench")
+    p.add_argument("--e2e-batch-jobs", type=int, default=32,
+                   help="GPU batch size of the end-to-end pass (the CLI's --gpu-batch-jobs): two batches in "
+                        "flight overlap one's upload and download with the other's kernels")
+    p.add_argument("--serve", action="store_true",
+                   help="serving run instead: Poisson arrivals through cs_submit / cs_poll, job latency")
+    p.add_argument("--serve-jobs", type=int, default=200)
+    p.add_argument("--serve-rate", type=float, default=50.0)
     return p.parse_args()
 
 
@@ -311,7 +322,8 @@ def run_b200(args):
     launches = prepared.launches * args.steps
 
     # End to end through the public API: plans in host memory, PCM back to host.
-    e2e_renderer = Renderer(device=local, natural=True, batch_jobs=len(plans))
+    e2e_batch = min(args.e2e_batch_jobs, len(plans)) if args.e2e_batch_jobs > 0 else len(plans)
+    e2e_renderer = Renderer(device=local, natural=True, batch_jobs=e2e_batch)
     e2e_renderer.upload_samples(bank)
     h2d = sum(p.spans.nbytes + p.points.nbytes + p.modulation.nbytes + p.track_offsets.nbytes for p in plans)
     box = {}
@@ -319,14 +331,15 @@ def run_b200(args):
     def publish(batch, first):
         # The PCM arrives in the renderer's page-locked buffer (the device-to-host
         # read of the step's result); the callback reads it in place.
-        box["pcm"] = batch.pcm.nbytes + batch.results.nbytes
-        box["audio"] = float(batch.results["frames"].sum()) / RATE
-        box["checksum"] = int(batch.pcm[::4096].astype(np.int64).sum())
+        box["pcm"] += batch.pcm.nbytes + batch.results.nbytes
+        box["audio"] += float(batch.results["frames"].sum()) / RATE
+        box["checksum"] += int(batch.pcm[::4096].astype(np.int64).sum())
 
     e2e_times = []
     for i in range(args.warmup + args.steps):
         barrier()
         torch.cuda.synchronize()
+        box.update(pcm=0, audio=0.0, checksum=0)
         start = time.perf_counter()
         e2e_renderer.render_window(plans, publish, copy=False)
         elapsed = time.perf_counter() - start
@@ -359,7 +372,8 @@ def run_b200(args):
                             "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                             "algorithmic_bytes": algorithmic[dominant], "traffic": traffic},
                "e2e": {"value": total_e2e_audio / max_e2e, "unit": "audio-s/s", "h2d_bytes_per_step": int(h2d),
-                       "d2h_bytes_per_step": int(box.get("pcm", 0)), "ms_per_step": max_e2e * 1e3},
+                       "d2h_bytes_per_step": int(box.get("pcm", 0)), "ms_per_step": max_e2e * 1e3,
+                       "batch_jobs": e2e_batch},
                "gpu_launches": launches, "clocks": clocks.summary()}
         if world == 1:
             try:
@@ -374,8 +388,83 @@ def run_b200(args):
         torch.distributed.destroy_process_group()
 
 
+def serving_requests(args, rank):
+    """The serving workload's plans (planned on the host), arrival times in seconds
+    and sample bank."""
+    from claysampler_b200 import workload as wl
+    from claysampler_b200.host import Host
+    root = args.workdir / f"serving_s{args.seed + rank}_j{args.serve_jobs}_r{args.serve_rate:g}"
+    marker = root / "ready"
+    if not marker.exists():
+        jobs, arrivals = wl.write_serving_jobs(root, seed=args.seed + rank, jobs=args.serve_jobs, rate=args.serve_rate)
+        marker.write_text("\n".join(f"{j.sfz}\t{j.midi}\t{float(t)!r}" for j, t in zip(jobs, arrivals)))
+    rows = [line.split("\t") for line in marker.read_text().splitlines()]
+    host = Host()
+    plans = [host.plan(Path(sfz), Path(midi), tail="natural") for sfz, midi, _ in rows]
+    arrivals = np.array([float(t) for _, _, t in rows])
+    bank = host.bank()
+    host.close()
+    return plans, arrivals, bank
+
+
+def run_serve(args):
+    """Render requests of the small kind (log-uniform 5-300 s over 8 presets)
+    arriving by a Poisson process, submitted one by one to a running renderer
+    (cs_submit) and published by cs_poll: continuous batching.  Reports the
+    submit-to-publish latency percentiles and the rendered audio-seconds per second;
+    each request is planned beforehand (CPU work outside the GPU path)."""
+    import torch
+    from claysampler_b200.renderer import Renderer
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    plans, arrivals, bank = serving_requests(args, rank)
+    plans = [p.pin() for p in plans]
+    renderer = Renderer(device=local, natural=True, batch_jobs=64)
+    renderer.upload_samples(bank)
+    done = {}
+
+    def publish(batch, first):
+        now = time.perf_counter()
+        for k, r in enumerate(batch.results):
+            done[first + k] = (now, float(r["frames"]) / RATE)
+
+    warm = min(8, len(plans))                  # warm-up: kernels, arenas, page-locked buffers
+    renderer.submit(plans[:warm])
+    while renderer.pending_jobs:
+        renderer.poll(publish, wait=True)
+    done.clear()
+    submitted = {}
+    start = time.perf_counter()
+    i = 0
+    while i < len(plans) or renderer.pending_jobs:
+        now = time.perf_counter() - start
+        while i < len(plans) and arrivals[i] <= now:
+            submitted[renderer.submit([plans[i]])] = time.perf_counter()
+            i += 1
+        if renderer.poll(publish, wait=i == len(plans)) == 0 and i < len(plans):
+            time.sleep(max(0.0, min(0.001, arrivals[i] - (time.perf_counter() - start))))
+    wall = time.perf_counter() - start
+    latency = np.array([1e3 * (done[t][0] - submitted[t]) for t in submitted])
+    audio = sum(done[t][1] for t in submitted)
+    offered = float(np.sum([p.frames for p in plans]) / RATE / arrivals[-1])
+    out = {"metric": "serving: submit-to-publish job latency, Poisson arrivals (continuous batching)",
+           "value": float(np.percentile(latency, 99)), "unit": "ms", "higher_is_better": False,
+           "p50_ms": float(np.percentile(latency, 50)), "p95_ms": float(np.percentile(latency, 95)),
+           "p99_ms": float(np.percentile(latency, 99)), "throughput_audio_s_per_s": audio / wall,
+           "offered_audio_s_per_s": offered, "jobs": len(submitted), "rate_jobs_per_s": args.serve_rate,
+           "wall_s": wall, "n_gpus": 1, "dtype": "f32", "data": "synthetic (seeded SFZ/WAV/MIDI)",
+           "config": {"workload": "requests of the small kind over 8 presets, lengths log-uniform 5-300 s",
+                      "batch_jobs": 64, "lanes": 2}}
+    if rank == 0:
+        print(json.dumps(out))
+    renderer.close()
+
+
 def main():
     args = parse()
+    if args.serve:
+        run_serve(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -13,8 +13,17 @@ constexpr int kTileFrames = 256;       // frames per mix tile (one voice list ea
 constexpr int kBlockFrames = CS_TAIL_BLOCK_FRAMES;
 constexpr int kTilesPerBlock = kBlockFrames / kTileFrames;
 constexpr int kSourceTile = 256;         // frames per source-kernel CTA
+#ifndef CS_SOURCE_THREADS
+#define CS_SOURCE_THREADS 128
+#endif
+constexpr int kSourceThreads = CS_SOURCE_THREADS;   // threads per source-kernel CTA
+static_assert(kSourceTile % kSourceThreads == 0, "whole frames per source thread");
 constexpr uint64_t kNoTargets = ~uint64_t(0);
 constexpr int kRecChainsPerCta = 32;     // single-slot chains per recurrence CTA
+#ifndef CS_LEAD_TIERS
+#define CS_LEAD_TIERS 3
+#endif
+constexpr int kLeadTiers = CS_LEAD_TIERS; // tiers of long chains whose recurrences start early
 // Moving-filter targets are stored per 32-frame chunk as three planes
 // (c0[32], c1[32], c2[32]) so the recurrence reads four frames per 128-bit load.
 constexpr int kRecChunkFrames = 32;

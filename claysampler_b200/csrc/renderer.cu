@@ -242,10 +242,13 @@ struct SegmentPlan {
     size_t scratchFloats, phaseFrames;
     size_t chainFirst, chainCount, simpleFirst, simpleCount, pitchFirst, pitchCount, blockFirst, blockCount;
     size_t tileFirst, tileCount;
-    // The longest single-slot chains and their source tiles come first: their
-    // recurrences start as soon as their sources are rendered, beside the sources
-    // and recurrences of the rest (0: no split).
-    size_t leadChains, leadTiles;
+    // The longest single-slot chains and their source tiles come first, in lead
+    // tiers of decreasing length: a tier's recurrences start as soon as its sources
+    // are rendered, beside the sources of the later tiers and the rest.  Tier k
+    // holds the chains of at least 1/2^(k+1) of the longest chain's frames;
+    // leadChains[k] / leadTiles[k] are its chain and source-tile counts (0: none).
+    int leadTiers;
+    size_t leadChains[kLeadTiers], leadTiles[kLeadTiers];
 };
 
 // Host side of a staged batch: segment boundaries and the per-segment arrays.
@@ -457,32 +460,38 @@ SegmentTables planSegments(const HostBatch& batch, size_t budget)
         // Longest recurrences first: neighbouring lanes then run similar lengths.
         std::stable_sort(simpleChains.begin(), simpleChains.end(),
                          [](const auto& x, const auto& y) { return x.first < y.first; });
-        // Lead chains: those at least half as long as the longest, in whole
-        // recurrence CTAs (measured on the 64-job batch against a quarter and a
-        // third: the rest's recurrences then still fit behind the rest's sources,
-        // and fewer lead CTAs share SMs with the source kernel).
-        size_t lead = 0;
+        // Lead tiers: tier k takes the chains of at least 1/2^(k+1) of the longest
+        // chain's frames, in whole recurrence CTAs; the rest's recurrences then run
+        // after all sources and are at most 1/2^kLeadTiers as long as the longest.
+        // A tier that would take every remaining chain is left to the rest.
+        seg.leadTiers = 0;
+        std::vector<unsigned char> tierOf(voiceCount, kLeadTiers);
+        size_t taken = 0;
         if (!simpleChains.empty()) {
             const long long longest = -simpleChains.front().first;
-            while (lead < simpleChains.size() && -simpleChains[lead].first * 2 >= longest)
-                ++lead;
-            lead = (lead + kRecChainsPerCta - 1) / kRecChainsPerCta * kRecChainsPerCta;
-            if (lead >= simpleChains.size())
-                lead = 0;
+            for (int k = 0; k < kLeadTiers; ++k) {
+                size_t end = taken;
+                while (end < simpleChains.size() && (-simpleChains[end].first << (k + 1)) >= longest)
+                    ++end;
+                end = (end + kRecChainsPerCta - 1) / kRecChainsPerCta * kRecChainsPerCta;
+                if (end >= simpleChains.size())
+                    break;
+                if (end == taken)
+                    continue;
+                for (size_t c = taken; c < end; ++c)
+                    tierOf[size_t(simpleChains[c].second)] = static_cast<unsigned char>(seg.leadTiers);
+                seg.leadChains[seg.leadTiers++] = end - taken;
+                taken = end;
+            }
         }
-        seg.leadChains = lead;
-        seg.leadTiles = 0;
-        // Source tiles: the lead chains' first, then the rest, each group in plan
-        // order (neighbouring tiles then read neighbouring samples and tracks).
-        std::vector<char> isLead(voiceCount, 0);
-        for (size_t k = 0; k < lead; ++k)
-            isLead[size_t(simpleChains[k].second)] = 1;
-        for (int group = lead ? 0 : 1; group < 2; ++group) {
-            if (group == 1)
-                seg.leadTiles = lead ? t.tileCount - seg.tileFirst : 0;
+        // Source tiles: tier by tier, then the rest, each group in plan order
+        // (neighbouring tiles then read neighbouring samples and tracks).
+        for (int group = 0; group <= seg.leadTiers; ++group) {
+            const size_t groupFirst = t.tileCount;
+            const int tier = group < seg.leadTiers ? group : kLeadTiers;
             for (const auto& item : simpleChains0) {
                 const int h = item.second;
-                if ((isLead[size_t(h)] != 0) != (group == 0))
+                if (tierOf[size_t(h)] != tier)
                     continue;
                 for (int span = h; span >= 0; span = batch.voices[size_t(span)].nextFilteredSpan) {
                     const auto& v = batch.voices[size_t(span)];
@@ -493,6 +502,8 @@ SegmentTables planSegments(const HostBatch& batch, size_t budget)
                     }
                 }
             }
+            if (group < seg.leadTiers)
+                seg.leadTiles[group] = t.tileCount - groupFirst;
         }
         seg.tileCount = t.tileCount - seg.tileFirst;
         if (t.tileCount > size_t(INT32_MAX))
@@ -569,11 +580,11 @@ struct cs_renderer {
     cs::TailConfig tail{};
     std::string name;
     cudaStream_t stream = nullptr;      // lane 0's stream
-    // A lane holds one batch in flight: its stream, a high-priority stream for the
-    // lead chains' recurrences, and the arena its batches reuse.
+    // A lane holds one batch in flight: its stream, a high-priority stream per lead
+    // tier for that tier's recurrences, and the arena its batches reuse.
     struct Lane {
-        cudaStream_t stream = nullptr, lead = nullptr;
-        cudaEvent_t leadReady = nullptr, leadDone = nullptr;
+        cudaStream_t stream = nullptr, lead[cs::kLeadTiers] = {};
+        cudaEvent_t leadReady[cs::kLeadTiers] = {}, leadDone[cs::kLeadTiers] = {};
         void* arena = nullptr;
         size_t arenaCapacity = 0;
     };
@@ -960,26 +971,31 @@ void run(cs_renderer& r, cs_prepared& p, cudaStream_t stream)
         launchPitch(view, s, stream);
         launches += s.pitchCount > 0;
         stage(0);
-        if (plan.leadChains) {
-            // Lead chains' sources, then their recurrences on the high-priority
-            // stream beside the rest of the sources and recurrences.
-            SegmentView lead = s, rest = s;
-            lead.sourceTileCount = int(plan.leadTiles);
-            lead.simpleCount = int(plan.leadChains);
-            rest.sourceTiles += plan.leadTiles;
-            rest.sourceTileCount -= int(plan.leadTiles);
-            rest.simple += plan.leadChains;
-            rest.simpleCount -= int(plan.leadChains);
-            launches += launchSources(view, lead, stream);
+        if (plan.leadTiers) {
+            // Each lead tier's sources, then its recurrences on that tier's
+            // high-priority stream beside the later tiers' and the rest's sources;
+            // the rest's recurrences last, then the join.
             const cs_renderer::Lane& lane = r.lanes[p.lane];
-            check(cudaEventRecord(lane.leadReady, stream), "CUDA event record");
-            check(cudaStreamWaitEvent(lane.lead, lane.leadReady, 0), "CUDA stream wait");
-            launches += launchRecurrences(view, lead, lane.lead);
-            check(cudaEventRecord(lane.leadDone, lane.lead), "CUDA event record");
+            SegmentView rest = s;
+            for (int k = 0; k < plan.leadTiers; ++k) {
+                SegmentView tier = rest;
+                tier.sourceTileCount = int(plan.leadTiles[k]);
+                tier.simpleCount = int(plan.leadChains[k]);
+                rest.sourceTiles += plan.leadTiles[k];
+                rest.sourceTileCount -= int(plan.leadTiles[k]);
+                rest.simple += plan.leadChains[k];
+                rest.simpleCount -= int(plan.leadChains[k]);
+                launches += launchSources(view, tier, stream);
+                check(cudaEventRecord(lane.leadReady[k], stream), "CUDA event record");
+                check(cudaStreamWaitEvent(lane.lead[k], lane.leadReady[k], 0), "CUDA stream wait");
+                launches += launchRecurrences(view, tier, lane.lead[k]);
+                check(cudaEventRecord(lane.leadDone[k], lane.lead[k]), "CUDA event record");
+            }
             launches += launchSources(view, rest, stream);
             stage(1);
             launches += launchRecurrences(view, rest, stream);
-            check(cudaStreamWaitEvent(stream, lane.leadDone, 0), "CUDA stream wait");
+            for (int k = 0; k < plan.leadTiers; ++k)
+                check(cudaStreamWaitEvent(stream, lane.leadDone[k], 0), "CUDA stream wait");
         } else {
             launches += launchSources(view, s, stream);
             stage(1);
@@ -1569,10 +1585,12 @@ int cs_renderer_create(int device, int natural, const cs_audio_config* audio, in
         cs::check(cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority), "CUDA stream priorities");
         for (auto& lane : r->lanes) {
             cs::check(cudaStreamCreateWithFlags(&lane.stream, cudaStreamNonBlocking), "CUDA stream");
-            cs::check(cudaStreamCreateWithPriority(&lane.lead, cudaStreamNonBlocking, greatestPriority),
-                      "CUDA stream");
-            cs::check(cudaEventCreateWithFlags(&lane.leadReady, cudaEventDisableTiming), "CUDA event");
-            cs::check(cudaEventCreateWithFlags(&lane.leadDone, cudaEventDisableTiming), "CUDA event");
+            for (int k = 0; k < cs::kLeadTiers; ++k) {
+                cs::check(cudaStreamCreateWithPriority(&lane.lead[k], cudaStreamNonBlocking, greatestPriority),
+                          "CUDA stream");
+                cs::check(cudaEventCreateWithFlags(&lane.leadReady[k], cudaEventDisableTiming), "CUDA event");
+                cs::check(cudaEventCreateWithFlags(&lane.leadDone[k], cudaEventDisableTiming), "CUDA event");
+            }
         }
         r->stream = r->lanes[0].stream;
         std::vector<float> table(size_t(cs::kTaps) * (cs::kPhases + 1));
@@ -1599,16 +1617,19 @@ void cs_renderer_destroy(cs_renderer* r)
     cudaFree(r->sinc);
     cudaFree(r->bank);
     for (auto& lane : r->lanes) {
-        if (lane.lead) cudaStreamSynchronize(lane.lead);
+        for (cudaStream_t lead : lane.lead)
+            if (lead) cudaStreamSynchronize(lead);
         cudaFree(lane.arena);
     }
     if (r->hostPcm) cudaFreeHost(r->hostPcm);
     if (r->staging) cudaFreeHost(r->staging);
     for (auto& lane : r->lanes) {
         if (lane.stream) cudaStreamDestroy(lane.stream);
-        if (lane.lead) cudaStreamDestroy(lane.lead);
-        if (lane.leadReady) cudaEventDestroy(lane.leadReady);
-        if (lane.leadDone) cudaEventDestroy(lane.leadDone);
+        for (int k = 0; k < cs::kLeadTiers; ++k) {
+            if (lane.lead[k]) cudaStreamDestroy(lane.lead[k]);
+            if (lane.leadReady[k]) cudaEventDestroy(lane.leadReady[k]);
+            if (lane.leadDone[k]) cudaEventDestroy(lane.leadDone[k]);
+        }
     }
     delete r;
 }

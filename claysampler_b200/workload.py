@@ -292,3 +292,24 @@ def write_uneven_batch(root: Path, seed: int = 3, jobs: int = 1024, presets: int
         _note_midi(notes, [], float(seconds), midi)
         out.append(Job("-", sfzs[j % presets], midi, root / "out" / f"uneven_{j:04d}.wav"))
     return out
+
+
+def write_serving_jobs(root: Path, seed: int = 5, jobs: int = 200, presets: int = 8, low: float = 5.0,
+                       high: float = 300.0, rate: float = 50.0) -> tuple[list[Job], np.ndarray]:
+    """Render requests of the serving kind: jobs over several presets of the small
+    kind, MIDI lengths log-uniform in [low, high] seconds at the small kind's note
+    density, arriving by a Poisson process of `rate` jobs per second.  Returns the
+    jobs and their arrival times in seconds."""
+    root.mkdir(parents=True, exist_ok=True)
+    sfzs = [write_plain_small_preset(root, seed + p, name=f"serve{p}") for p in range(presets)]
+    rng = np.random.default_rng(seed + 2000)
+    lengths = np.exp(rng.uniform(np.log(low), np.log(high), jobs))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, jobs))
+    out = []
+    for j, seconds in enumerate(lengths):
+        count = max(1, int(round(64 * seconds / 30.0)))
+        notes = _performance(rng, float(seconds), None, count, 40, 120, 0.5)
+        midi = root / f"serve_{j:04d}.mid"
+        _note_midi(notes, [], float(seconds), midi)
+        out.append(Job("-", sfzs[j % presets], midi, root / "out" / f"serve_{j:04d}.wav"))
+    return out, arrivals

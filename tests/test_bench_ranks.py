@@ -70,3 +70,23 @@ def test_each_rank_renders_its_own_batch(tmp_path, monkeypatch):
     args = argparse.Namespace(workdir=tmp_path, seed=2, jobs=1)
     a, b = bench.workload(args, 0), bench.workload(args, 1)
     assert seeds == [2, 3] and a != b
+
+
+def test_serving_requests(tmp_path):
+    """The serving workload: seeded requests of the small kind with lengths in
+    [5, 300] s, arriving in increasing order (a Poisson process of the given rate),
+    planned by the host planner."""
+    import argparse
+    sys.path.insert(0, str(ROOT))
+    import bench
+    args = argparse.Namespace(workdir=tmp_path, seed=5, serve_jobs=6, serve_rate=50.0)
+    plans, arrivals, bank = bench.serving_requests(args, 0)
+    again, arrivals_again, _ = bench.serving_requests(args, 0)
+    assert len(plans) == 6 and bank.size > 0
+    assert np.all(np.diff(arrivals) > 0) and arrivals[0] > 0
+    assert np.array_equal(arrivals, arrivals_again)
+    assert [p.frames for p in plans] == [p.frames for p in again]
+    seconds = np.array([p.music_end for p in plans]) / 44100
+    assert np.all(seconds >= 4.5) and np.all(seconds <= 300.5)
+    other, arrivals_other, _ = bench.serving_requests(args, 1)
+    assert not np.array_equal(arrivals, arrivals_other)
