@@ -286,35 +286,37 @@ __device__ __forceinline__ void sourceFrame(const BatchView& b, const SegmentVie
 {
     const cs_voice_span& v = b.voices[span];
     const int start = max(v.begin, s.first);
-    const double position = v.variablePitch ? b.phase[s.phaseOffset[span] + (frame - start)] : -1.0;
     const int* tracks = v.filterControls;
     const float pan = trackAt(b.points, tracks[2], tracks[3], frame);
-    const float2 sample = voiceFrame(b.bank, b.sinc, v, b.points, b.modulation, pan, frame, true, position);
+    const uint64_t targets = s.targetOffset[span];
+    const int f = targets == kNoTargets ? -1 : activeSlot(v);
+    // voiceFrame and filterTargetSlot with one walk over the bindings; the filter
+    // targets first, so that their sums are dead before the voice is rendered.
+    const float level = envelopeAt(v, frame);
+    const SourceMods mods = sourceMods(v, b.points, b.modulation, level, pan, frame, f);
+    if (f >= 0 && (mods.moving || frame == v.begin)) {
+        const Compact c = compactOf(v.filters[f].type, filterFromMods(v, f, mods.filter, frame));
+        if (mods.moving) {
+            const int rel = frame - start;
+            float* out = b.filtered + targets + size_t(rel / kRecChunkFrames) * 3 * kRecChunkFrames + rel % kRecChunkFrames;
+            out[0] = c.c0;
+            out[kRecChunkFrames] = c.c1;
+            out[2 * kRecChunkFrames] = c.c2;
+        } else {
+            float* out = b.filtered + targets;
+            out[0] = c.c0;
+            out[1] = c.c1;
+            out[2] = c.c2;
+        }
+    }
+    const double position = v.variablePitch ? b.phase[s.phaseOffset[span] + (frame - start)] : -1.0;
+    const float2 sample = level <= 0 ? make_float2(0.f, 0.f)
+                                     : voiceOutput(b.bank, b.sinc, v, mods.voice, frame, true, position);
     const float gain = jobGainAt(b.points, tracks, frame);
     float* dst = b.filtered + s.scratchOffset[span] + size_t(frame - start) * v.channels;
     dst[0] = sample.x * gain;
     if (v.channels == 2)
         dst[1] = sample.y * gain;
-    const uint64_t targets = s.targetOffset[span];
-    if (targets == kNoTargets)
-        return;
-    const bool moving = filterMoves(v, b.modulation);
-    if (!moving && frame != v.begin)
-        return;
-    const int f = activeSlot(v);
-    const Compact c = compactOf(v.filters[f].type, filterTargetSlot(v, b.points, b.modulation, frame, f));
-    if (moving) {
-        const int rel = frame - start;
-        float* out = b.filtered + targets + size_t(rel / kRecChunkFrames) * 3 * kRecChunkFrames + rel % kRecChunkFrames;
-        out[0] = c.c0;
-        out[kRecChunkFrames] = c.c1;
-        out[2 * kRecChunkFrames] = c.c2;
-    } else {
-        float* out = b.filtered + targets;
-        out[0] = c.c0;
-        out[1] = c.c1;
-        out[2] = c.c2;
-    }
 }
 
 // Shared-memory carveout (percent of the maximum) of the source and recurrence

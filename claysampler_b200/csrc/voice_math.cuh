@@ -448,6 +448,40 @@ __device__ __forceinline__ Biquad filterFromMods(const cs_voice_span& v, int f, 
     return designFilter(filter.type, filter.cutoff * exp2f(cents / 1200), filter.resonance + s.db, v.sampleRate, 0, 0);
 }
 
+// The modulation sums of one frame of a filtered voice, for its output and for the
+// target coefficients of its filter slot `f` (-1: none), in one pass over its
+// bindings: each binding's value is computed once and added to the sum it feeds,
+// and every sum keeps the reference's binding order (render.cu:138-160, 370-396).
+// `moving` is filterMoves for the span.
+struct SourceMods {
+    VoiceMods voice;
+    FilterMods filter;
+    bool moving;
+};
+
+__device__ __forceinline__ SourceMods sourceMods(const cs_voice_span& v, const cs_control_point* __restrict__ points,
+                                                 const cs_voice_modulation* __restrict__ modulation, float level,
+                                                 float pan, int frame, int f)
+{
+    SourceMods s{{level, 0.f, pan, 0.f, 0.f}, {0.f, 0.f, v.extraEnvelope[0].depth}, v.activeEnvelope[0] != 0};
+    const int end = v.firstModulation + v.modulationCount;
+    for (int j = v.firstModulation; j < end; ++j) {
+        const int target = modulation[j].target;
+        s.moving |= (target >= CS_MOD_CUTOFF && target <= CS_MOD_RESONANCE2) || target == CS_MOD_FILEG_DEPTH ||
+            target >= CS_MOD_EQ1_FREQUENCY;
+        const bool voice = target <= CS_MOD_POSITION;
+        const bool filter = f >= 0 && filterModTarget(f, target);
+        if (!voice && !filter)
+            continue;
+        const float value = bindingAt(modulation[j], points, frame);
+        if (voice)
+            addVoiceMod(s.voice, target, value);
+        else
+            addFilterMod(s.filter, f, target, value);
+    }
+    return s;
+}
+
 // Target coefficients of one of the two main filter slots at `frame`; the same
 // accumulation as filterTargets restricted to slot `f` (render.cu:378-404).
 __device__ __forceinline__ Biquad filterTargetSlot(const cs_voice_span& v, const cs_control_point* __restrict__ points,
