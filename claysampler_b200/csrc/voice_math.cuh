@@ -171,6 +171,19 @@ __device__ __forceinline__ float2 sincAt(const float* __restrict__ bank, const f
     return make_float2(x, y);
 }
 
+// fmod(x, period), which is exact.  For 0 <= x < 2^32 and a positive period it is
+// the remainder of x's whole part (a 32-bit integer remainder) plus x's fraction:
+// x - floor(x) is exact, and the sum is the exact remainder, so it is returned
+// unrounded.  Other arguments go to fmod.
+__device__ __forceinline__ double loopRemainder(double x, int period)
+{
+    if (x >= 0 && x < 4294967296.0 && period > 0) {
+        const double whole = floor(x);
+        return double(unsigned(whole) % unsigned(period)) + (x - whole);
+    }
+    return fmod(x, double(period));
+}
+
 // Source value of a voice at output `frame` (render.cu:63-100): position from the
 // span's start (or a precomputed variable-pitch phase), generators, loop wrap and
 // loop crossfade.
@@ -199,7 +212,7 @@ __device__ __forceinline__ float2 voiceSource(const float* __restrict__ bank, co
     }
     const int period = v.loopEnd - v.loopFirst;
     if (v.loopEnd > 0 && pos >= v.loopEnd)
-        pos = v.loopFirst + fmod(pos - v.loopFirst, double(period));
+        pos = v.loopFirst + loopRemainder(pos - v.loopFirst, period);
     if (pos >= v.sourceEnd)
         return make_float2(0.f, 0.f);
     float2 sample = sincAt(bank, sinc, v, pos);

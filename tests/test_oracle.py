@@ -61,3 +61,23 @@ def test_restated_render_pitch_and_bends(tmp_path, ref_session):
         theirs = reference.synthesize(plans, bank, natural)
         mine = oracle.synthesize(plans, bank, natural)
         assert np.array_equal(mine.view(np.uint32 if natural else np.uint16), theirs.view(np.uint32 if natural else np.uint16))
+
+
+def test_loop_remainder_identity_is_exact():
+    """The device's loop wrap computes fmod(x, period) as the remainder of x's whole
+    part plus x's fraction (voice_math.cuh, loopRemainder).  Both parts are exact in
+    IEEE double and their sum is the exact remainder, so the result equals fmod's
+    bit for bit; checked here on the positions a loop wrap sees (whole and
+    fractional, near period multiples, up to 2^32)."""
+    rng = np.random.default_rng(7)
+    periods = np.concatenate([rng.integers(1, 1 << 20, 4000), [1, 2, 3, 1023, 65536, (1 << 31) - 1]])
+    whole = rng.integers(0, 1 << 32, periods.size).astype(np.float64)
+    frac = rng.random(periods.size)
+    for x in (whole, whole + frac, np.minimum(whole + 0.999999999, 4294967295.0),
+              periods * rng.integers(1, 50, periods.size) + frac,
+              periods * rng.integers(1, 50, periods.size) - 2.0 ** -20):
+        x = x[(x >= 0) & (x < 2.0 ** 32)]
+        p = periods[: x.size]
+        floor = np.floor(x)
+        restated = (floor.astype(np.uint64) % p.astype(np.uint64)).astype(np.float64) + (x - floor)
+        assert np.array_equal(restated.view(np.uint64), np.fmod(x, p.astype(np.float64)).view(np.uint64))
