@@ -747,6 +747,10 @@ __global__ void __launch_bounds__(kMixThreads, Inline ? 5 : 8) mixKernel(BatchVi
     // frame's walk over its voices reads shared memory and then the voice's samples.
     __shared__ MixVoice staged[kTilesPerBlock][kMixStaged];
     __shared__ MixTile tiles[kTilesPerBlock];
+    __shared__ int mixedTiles;          // bit k: tile k is not all staged stereo filtered voices
+    if (threadIdx.x == 0)
+        mixedTiles = 0;
+    __syncthreads();
     const int block = s.blocks[blockIdx.x];
     const int jobIndex = b.blockJob[block];
     const JobInfo job = b.jobs[jobIndex];
@@ -756,8 +760,11 @@ __global__ void __launch_bounds__(kMixThreads, Inline ? 5 : 8) mixKernel(BatchVi
         const int k = int(threadIdx.x) / kMixStaged, i = int(threadIdx.x) % kMixStaged;
         const int tileIndex = local * kTilesPerBlock + k;
         const MixTile tile = tileIndex < jobTiles ? b.tiles[job.tileFirst + tileIndex] : MixTile{0, 0};
-        if (i == 0)
+        if (i == 0) {
             tiles[k] = tile;
+            if (tile.count > kMixStaged)
+                atomicOr(&mixedTiles, 1 << k);
+        }
         if (i < tile.count && tile.count <= kMixStaged) {
             const int index = __ldg(b.indices + tile.first + i);
             const cs_voice_span& v = b.voices[index];
@@ -772,6 +779,8 @@ __global__ void __launch_bounds__(kMixThreads, Inline ? 5 : 8) mixKernel(BatchVi
                 m.kind = 0;
                 m.offset = 0;
             }
+            if (m.kind != 1)
+                atomicOr(&mixedTiles, 1 << k);
             staged[k][i] = m;
         }
     }
@@ -812,7 +821,30 @@ __global__ void __launch_bounds__(kMixThreads, Inline ? 5 : 8) mixKernel(BatchVi
                 right += sample.y;
             }
         };
-        if (tile.count <= kMixStaged) {
+        if (!(mixedTiles >> k & 1)) {
+            // Stereo filtered voices only: four voices' frames loaded at a time, then
+            // added in span order, so more loads are in flight per thread.
+            int i = 0;
+            for (; i + 4 <= tile.count; i += 4) {
+                float2 sample[4];
+                bool live[4];
+                #pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const MixVoice& m = staged[k][i + u];
+                    live[u] = frame >= m.begin && frame < m.end;
+                    sample[u] = live[u] ? *reinterpret_cast<const float2*>(b.filtered + (m.offset + 2ll * frame))
+                                        : make_float2(0.f, 0.f);
+                }
+                #pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (live[u]) {
+                        wetLeft += sample[u].x;
+                        wetRight += sample[u].y;
+                    }
+            }
+            for (; i < tile.count; ++i)
+                addVoice(staged[k][i]);
+        } else if (tile.count <= kMixStaged) {
             for (int i = 0; i < tile.count; ++i)
                 addVoice(staged[k][i]);
         } else {
