@@ -61,6 +61,10 @@ def parse():
                         "flight overlap one's upload and download with the other's kernels")
     p.add_argument("--serve", action="store_true",
                    help="serving run instead: Poisson arrivals through cs_submit / cs_poll, job latency")
+    p.add_argument("--learned", action="store_true",
+                   help="train the note-lifetime predictor on single-note renders and report it")
+    p.add_argument("--learned-jobs", type=int, default=2048, help="training jobs of 64 isolated notes each")
+    p.add_argument("--learned-epochs", type=int, default=30)
     p.add_argument("--serve-jobs", type=int, default=200)
     p.add_argument("--serve-rate", type=float, default=50.0)
     return p.parse_args()
@@ -460,8 +464,72 @@ def run_serve(args):
     renderer.close()
 
 
+def run_learned(args):
+    """The learned part end to end on one GPU: single-note renders by the renderer label
+    a training set (audible frames at -90 dBFS and peak), the MLP is trained by the
+    library's fused forward/backward + Adam kernels, and held-out notes (the last 10 %
+    of the jobs) compare its predictions and its lifetime reservation with the plain
+    estimate (the planner's release bound, velocity gain)."""
+    import torch
+    from claysampler_b200 import lifetime
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    root = args.workdir / f"learned_s{args.seed + rank}_j{args.learned_jobs}"
+    root.mkdir(parents=True, exist_ok=True)
+    t0 = time.perf_counter()
+    features, targets, spans, job = lifetime.render_training_set(root, seed=args.seed + rank,
+                                                                 jobs=args.learned_jobs, notes=64,
+                                                                 batch_jobs=128, device=f"cuda:{local}")
+    label_s = time.perf_counter() - t0
+    cut = int(round(0.9 * args.learned_jobs))
+    train, test = job < cut, job >= cut
+    net = lifetime.LifetimeNet(device=f"cuda:{local}", seed=args.seed)
+    net.set_normalisation(lifetime.normalisation(features[train], targets[train]))
+    net.train(features[train][:4096], targets[train][:4096], epochs=1, batch=4096)   # warm-up
+    net = lifetime.LifetimeNet(device=f"cuda:{local}", seed=args.seed)
+    net.set_normalisation(lifetime.normalisation(features[train], targets[train]))
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record()
+    history = net.train(features[train], targets[train], epochs=args.learned_epochs, batch=4096, rate=3e-3,
+                        decay=0.9)
+    end.record()
+    torch.cuda.synchronize()
+    train_ms = start.elapsed_time(end)
+    predicted = net.predict(features[test]).cpu().numpy()
+    plain = lifetime.envelope_estimate(features[test])
+    truth = targets[test]
+    audible = np.exp(truth[:, 0]).round().astype(np.int64)
+    reserve_net = lifetime.admission_reservation(predicted[:, 0])
+    reserve_plain = np.exp(plain[:, 0]).round().astype(np.int64)
+    out = {"metric": "learned note lifetime / peak: held-out mean absolute error and lifetime reservation",
+           "value": float(np.abs(predicted[:, 0] - truth[:, 0]).mean()), "unit": "|log audible frames| error",
+           "higher_is_better": False,
+           "mae_log_frames": {"network": float(np.abs(predicted[:, 0] - truth[:, 0]).mean()),
+                              "plain": float(np.abs(plain[:, 0] - truth[:, 0]).mean())},
+           "mae_peak_db": {"network": float(np.abs(predicted[:, 1] - truth[:, 1]).mean()),
+                           "plain": float(np.abs(plain[:, 1] - truth[:, 1]).mean())},
+           "reserved_frames": {"network": int(reserve_net.sum()), "plain": int(reserve_plain.sum()),
+                               "audible": int(audible.sum()), "rendered_spans": int(spans[test].sum())},
+           "reservation_cut": float(1 - reserve_net.sum() / reserve_plain.sum()),
+           "mispredict_rate": {"network": float(np.mean(audible > reserve_net)),
+                               "plain": float(np.mean(audible > reserve_plain))},
+           "train_notes": int(train.sum()), "test_notes": int(test.sum()), "epochs": args.learned_epochs,
+           "loss_first_last": [history[0], history[-1]],
+           "train_ms": train_ms, "train_samples_per_s": 1e3 * args.learned_epochs * int(train.sum()) / train_ms,
+           "label_render_s": label_s, "n_gpus": 1, "dtype": "bf16 weights, f32 accumulate",
+           "data": "synthetic (seeded random regions, single-note MIDI)",
+           "config": {"workload": "MLP 16-64-64-2 on single-note renders, 4 instruments x 88 random regions",
+                      "batch": 4096, "margin": 1.25, "threshold_dbfs": lifetime.AUDIBLE_DBFS}}
+    if rank == 0:
+        print(json.dumps(out))
+
+
 def main():
     args = parse()
+    if args.learned:
+        run_learned(args)
+        return
     if args.serve:
         run_serve(args)
         return

@@ -44,7 +44,8 @@ def _run(cmd: list[str]) -> None:
 
 def build_library(force: bool = False, verbose: bool = False) -> Path:
     sources = sorted(CSRC.glob("*.cu"))
-    deps = sources + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.hpp")) + [ROOT / "include" / "claysampler_b200.h"]
+    deps = (sources + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.hpp"))
+            + [ROOT / "include" / "claysampler_b200.h", ROOT / "include" / "claysampler_lifetime.h"])
     if force or _stale(LIBRARY, deps):
         tmp = LIBRARY.with_suffix(f".so.tmp{os.getpid()}")
         cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC,-O2",

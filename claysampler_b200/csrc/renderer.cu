@@ -1721,6 +1721,16 @@ int cs_copy_mix(cs_renderer* r, cs_prepared* p, void* host, size_t bytes)
 
 size_t cs_prepared_frames(const cs_prepared* p) { return p ? p->batch.frames : 0; }
 
+int cs_prepared_mix_device(const cs_prepared* p, const void** mix, size_t* bytes)
+{
+    return cs::guarded([&] {
+        if (!p || !mix || !bytes)
+            throw std::runtime_error("null argument");
+        *mix = p->view.mix;
+        *bytes = p->mixBytes;
+    });
+}
+
 int cs_prepared_set_profile(cs_prepared* p, int enable)
 {
     return cs::guarded([&] {

@@ -235,6 +235,9 @@ int cs_collect(cs_renderer* renderer, cs_prepared* batch, int16_t* pcm, size_t p
  * for all jobs, concatenated in plan order. */
 int cs_copy_mix(cs_renderer* renderer, cs_prepared* batch, void* host, size_t bytes);
 size_t cs_prepared_frames(const cs_prepared* batch);
+/* Device address and size of that mix, valid until the batch is destroyed or run
+ * again; the caller orders its reads after cs_run's work (same stream, or an event). */
+int cs_prepared_mix_device(const cs_prepared* batch, const void** mix, size_t* bytes);
 /* Kernel launches the last cs_run enqueued. */
 int cs_prepared_launches(const cs_prepared* batch);
 void cs_prepared_destroy(cs_prepared* batch);
