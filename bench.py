@@ -44,6 +44,11 @@ sys.path.insert(0, str(ROOT))
 RATE = 44100
 METRIC = "audio-sec/sec on 1 B200 (batched+learned vs plain, ≤1 LSB); HBM GB/s; p99"
 WORKLOAD = "plain batch: 64 jobs, 88 keys x 4 layers stereo 24-bit, lpf_2p + fileg + 5 Hz LFO, loops, pedal"
+WORKLOADS = {
+    "plain_batch": WORKLOAD,
+    "uneven": "uneven batch: 1024 jobs over 4 presets of 12 mono 16-bit regions (48-tap sinc resampling, "
+              "no filter), Pareto(1.5) lengths 2-600 s",
+}
 
 
 def parse():
@@ -52,7 +57,9 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    p.add_argument("--jobs", type=int, default=64)
+    p.add_argument("--workload", choices=sorted(WORKLOADS), default="plain_batch",
+                   help="plain_batch: the 64-job filtered batch; uneven: 1024 Pareto-length jobs")
+    p.add_argument("--jobs", type=int, default=None, help="jobs per rank (default 64, or 1024 for uneven)")
     p.add_argument("--seed", type=int, default=2)
     p.add_argument("--cpu-sample-jobs", type=int, default=32)
     p.add_argument("--workdir", type=Path, default=Path(tempfile.gettempdir()) / "claysampler_bench")
@@ -65,6 +72,8 @@ def parse():
                    help="train the note-lifetime predictor on single-note renders and report it")
     p.add_argument("--learned-jobs", type=int, default=2048, help="training jobs of 64 isolated notes each")
     p.add_argument("--learned-epochs", type=int, default=30)
+    p.add_argument("--learned-mispredict", type=float, default=0.01,
+                   help="mispredict rate the reservation margin is calibrated to on the training notes")
     p.add_argument("--serve-jobs", type=int, default=200)
     p.add_argument("--serve-rate", type=float, default=50.0)
     return p.parse_args()
@@ -79,10 +88,16 @@ def dist_info():
 
 def workload(args, rank):
     from claysampler_b200 import workload as wl
-    root = args.workdir / f"plain_batch_s{args.seed + rank}_j{args.jobs}"
+    kind = getattr(args, "workload", "plain_batch")
+    if args.jobs is None:
+        args.jobs = 1024 if kind == "uneven" else 64
+    root = args.workdir / f"{kind}_s{args.seed + rank}_j{args.jobs}"
     marker = root / "ready"
     if not marker.exists():
-        jobs = wl.write_plain_batch(root, seed=args.seed + rank, jobs=args.jobs)
+        if kind == "uneven":
+            jobs = wl.write_uneven_batch(root, seed=args.seed + rank, jobs=args.jobs)
+        else:
+            jobs = wl.write_plain_batch(root, seed=args.seed + rank, jobs=args.jobs)
         marker.write_text("\n".join(f"{j.sfz}\t{j.midi}" for j in jobs))
     return [tuple(map(Path, line.split("\t"))) for line in marker.read_text().splitlines()]
 
@@ -267,7 +282,8 @@ def run_reference(args):
     out = {"metric": METRIC, "value": value, "unit": "audio-s/s", "n_gpus": args.gpus, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SFZ/WAV/MIDI)", "impl": "reference",
-           "config": {"workload": WORKLOAD, "sample": f"first {len(sample)} jobs", "tail": "natural"},
+           "config": {"workload": WORKLOADS[args.workload], "sample": f"first {len(sample)} jobs",
+                      "tail": "natural"},
            "cpu_baseline": {"value": value, "unit": "audio-s/s", "cores": threads, "kind": kind,
                             "sample": f"first {len(sample)} of {len(plans)} jobs per step"},
            "e2e": {"value": value, "unit": "audio-s/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -367,7 +383,7 @@ def run_b200(args):
         out = {"metric": METRIC, "value": total_audio / (max_ms * 1e-3), "unit": "audio-s/s", "n_gpus": world,
                "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SFZ/WAV/MIDI)",
-               "config": {"workload": WORKLOAD, "jobs_per_gpu": len(plans), "seed": args.seed,
+               "config": {"workload": WORKLOADS[args.workload], "jobs_per_gpu": len(plans), "seed": args.seed,
                           "output_audio_s_per_gpu": audio, "voice_frames_per_gpu": voice_frames,
                           "tail": "natural", "taps": 48, "l2": "inputs larger than L2 (no flush)",
                           "parallelism": f"jobs sharded by rank, {world} rank(s)", "statuses": statuses},
@@ -496,12 +512,14 @@ def run_learned(args):
     end.record()
     torch.cuda.synchronize()
     train_ms = start.elapsed_time(end)
+    margin = lifetime.calibrate_margin(net.predict(features[train]).cpu().numpy()[:, 0], targets[train][:, 0],
+                                       args.learned_mispredict)
     predicted = net.predict(features[test]).cpu().numpy()
     plain = lifetime.envelope_estimate(features[test])
     truth = targets[test]
     audible = np.exp(truth[:, 0]).round().astype(np.int64)
-    reserve_net = lifetime.admission_reservation(predicted[:, 0])
-    reserve_plain = np.exp(plain[:, 0]).round().astype(np.int64)
+    reserve_net = lifetime.admission_reservation(predicted[:, 0], plain[:, 0], margin)
+    reserve_plain = np.ceil(np.exp(plain[:, 0])).astype(np.int64)
     out = {"metric": "learned note lifetime / peak: held-out mean absolute error and lifetime reservation",
            "value": float(np.abs(predicted[:, 0] - truth[:, 0]).mean()), "unit": "|log audible frames| error",
            "higher_is_better": False,
@@ -520,7 +538,9 @@ def run_learned(args):
            "label_render_s": label_s, "n_gpus": 1, "dtype": "bf16 weights, f32 accumulate",
            "data": "synthetic (seeded random regions, single-note MIDI)",
            "config": {"workload": "MLP 16-64-64-2 on single-note renders, 4 instruments x 88 random regions",
-                      "batch": 4096, "margin": 1.25, "threshold_dbfs": lifetime.AUDIBLE_DBFS}}
+                      "batch": 4096, "margin_log_frames": margin,
+                      "calibrated_mispredict_rate": args.learned_mispredict,
+                      "threshold_dbfs": lifetime.AUDIBLE_DBFS}}
     if rank == 0:
         print(json.dumps(out))
 

@@ -8,12 +8,15 @@ on the GPU by the library's own fused forward/backward and Adam kernels, on labe
 measured from single-note renders made by the renderer itself
 (:func:`render_training_set`).
 
-The predictor never touches audio.  Every job is still finished by the plain tail
-detection, so PCM is identical with or without it.  What it sizes is the
-reservation made for a job at admission, before the job is planned
-(:func:`admission_reservation`); once the job is planned its exact footprint is
-known, and a job whose footprint exceeds what was reserved for it is a mispredict:
-it waits until the exact amount is free (the plain method's fallback).
+The predictor never touches audio: no render path reads it, and every job is still
+finished by the plain tail detection, so PCM is identical with or without it.
+:func:`admission_reservation` turns a prediction into a per-note frame
+reservation (raised by a margin calibrated on the training notes, capped by the
+planner's own bound), and ``bench.py --learned`` reports how much less that
+reserves than the plain bound and how often a note outlives its reservation.  The
+renderer itself keeps reserving exactly what the plan needs: it renders every span
+in full (that is what keeps PCM bit-identical), so a shorter predicted lifetime
+cannot shrink its scratch without changing what is rendered.
 
 Everything device-side goes through the C ABI with plain device pointers; torch is
 only the allocator for those buffers.
@@ -415,6 +418,15 @@ def envelope_estimate(features: np.ndarray) -> np.ndarray:
     return np.stack([np.log(np.maximum(length * RATE, 1)), 40 * np.log10(velocity)], axis=1)
 
 
-def admission_reservation(log_frames: np.ndarray, margin: float = 1.25) -> np.ndarray:
-    """Frames reserved per note from a predicted log lifetime, with a safety margin."""
-    return np.ceil(np.exp(np.asarray(log_frames, np.float64)) * margin).astype(np.int64)
+def calibrate_margin(predicted_log: np.ndarray, true_log: np.ndarray, mispredict_rate: float = 0.01) -> float:
+    """Log-frame margin above the prediction that covers all but `mispredict_rate` of the
+    calibration notes (a quantile of their residuals)."""
+    residual = np.asarray(true_log, np.float64) - np.asarray(predicted_log, np.float64)
+    return float(np.quantile(residual, 1.0 - mispredict_rate))
+
+
+def admission_reservation(predicted_log: np.ndarray, plain_log: np.ndarray, margin_log: float) -> np.ndarray:
+    """Frames reserved per note: the prediction raised by the calibrated margin, never more
+    than the plain estimate (the planner's bound on the note's render length)."""
+    predicted = np.exp(np.asarray(predicted_log, np.float64) + margin_log)
+    return np.ceil(np.minimum(predicted, np.exp(np.asarray(plain_log, np.float64)))).astype(np.int64)

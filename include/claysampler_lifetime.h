@@ -1,10 +1,11 @@
 /*
  * claysampler_b200 note-lifetime predictor — a small MLP that predicts, from a
  * note's region parameters, velocity, key and held time, how long the note stays
- * audible and how loud it peaks.  The renderer never uses it to decide audio: the
- * plain tail detection judges every job, so output PCM is the same with or without
- * the predictor.  It only sizes reservations made before a job is planned
- * (admission), and its mispredicts there are caught once the job is planned.
+ * audible and how loud it peaks.  No render path reads it: the plain tail
+ * detection judges every job, so output PCM is the same with or without the
+ * predictor.  Its predictions size per-note lifetime reservations on the host
+ * side (claysampler_b200/lifetime.py), which report how much a renderer that ends
+ * voices at their audible end could save.
  *
  * No counterpart in the reference: ClaySampler decides every length after
  * rendering (the natural endpoint search, src/cuda/tail.cu:83-139) and sizes its
