@@ -12,9 +12,15 @@ natural-tail finishing to packed mono PCM16.  `value` times steps on inputs that
 are already resident in device memory (bank 497 MB and per-step scratch well
 above the 126 MB L2, so no flush is needed); `e2e` times the public
 render_window call with the plans in host memory, including the plan upload and
-the PCM download (GPU batches of 32 jobs, the CLI's --gpu-batch-jobs, so that two
-batches in flight overlap their transfers with each other's kernels).  Under
-torchrun every rank renders its own batch (no collective), so scaling is weak.
+the PCM download, in GPU batches (the CLI's --gpu-batch-jobs) whose size the
+autotuner (claysampler_b200/autotune.py) measured fastest for the workload, so
+that two batches in flight overlap their transfers with each other's kernels.
+Under torchrun every rank renders its own batch (no collective), so scaling is
+weak.
+
+`--workload uneven` renders instead the 1024-job batch of Pareto(1.5) lengths
+(four presets of the small mono kind, 48-tap sinc resampling on most voices).
+`--learned` trains and scores the note-lifetime predictor.
 
 `--serve` measures instead the submit-to-publish latency of requests that arrive
 one at a time (Poisson) through the non-blocking submit / poll pair.
@@ -66,12 +72,16 @@ def parse():
     p.add_argument("--e2e-batch-jobs", type=int, default=32,
                    help="GPU batch size of the end-to-end pass (the CLI's --gpu-batch-jobs): two batches in "
                         "flight overlap one's upload and download with the other's kernels")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="skip the GPU batch-size sweep and use --e2e-batch-jobs for the end-to-end pass")
     p.add_argument("--serve", action="store_true",
                    help="serving run instead: Poisson arrivals through cs_submit / cs_poll, job latency")
     p.add_argument("--learned", action="store_true",
                    help="train the note-lifetime predictor on single-note renders and report it")
     p.add_argument("--learned-jobs", type=int, default=2048, help="training jobs of 64 isolated notes each")
     p.add_argument("--learned-epochs", type=int, default=30)
+    p.add_argument("--learned-preset-jobs", type=int, default=128,
+                   help="jobs of 64 isolated notes of the 64-job batch's preset to score the network on")
     p.add_argument("--learned-mispredict", type=float, default=0.01,
                    help="mispredict rate the reservation margin is calibrated to on the training notes")
     p.add_argument("--serve-jobs", type=int, default=200)
@@ -341,8 +351,14 @@ def run_b200(args):
     ms = sum(step_ms) / len(step_ms)
     launches = prepared.launches * args.steps
 
-    # End to end through the public API: plans in host memory, PCM back to host.
+    # End to end through the public API: plans in host memory, PCM back to host, in
+    # GPU batches of the size the autotuner measured fastest for this workload.
     e2e_batch = min(args.e2e_batch_jobs, len(plans)) if args.e2e_batch_jobs > 0 else len(plans)
+    tuned = None
+    if not getattr(args, "no_autotune", False):
+        from claysampler_b200 import autotune
+        tuned = autotune.tune(plans, bank, device=local, cache=args.workdir / "autotune.json")
+        e2e_batch = tuned["batch_jobs"]
     e2e_renderer = Renderer(device=local, natural=True, batch_jobs=e2e_batch)
     e2e_renderer.upload_samples(bank)
     h2d = sum(p.spans.nbytes + p.points.nbytes + p.modulation.nbytes + p.track_offsets.nbytes for p in plans)
@@ -393,7 +409,7 @@ def run_b200(args):
                             "algorithmic_bytes": algorithmic[dominant], "traffic": traffic},
                "e2e": {"value": total_e2e_audio / max_e2e, "unit": "audio-s/s", "h2d_bytes_per_step": int(h2d),
                        "d2h_bytes_per_step": int(box.get("pcm", 0)), "ms_per_step": max_e2e * 1e3,
-                       "batch_jobs": e2e_batch},
+                       "batch_jobs": e2e_batch, "autotune": tuned},
                "gpu_launches": launches, "clocks": clocks.summary()}
         if world == 1:
             try:
@@ -520,6 +536,32 @@ def run_learned(args):
     audible = np.exp(truth[:, 0]).round().astype(np.int64)
     reserve_net = lifetime.admission_reservation(predicted[:, 0], plain[:, 0], margin)
     reserve_plain = np.ceil(np.exp(plain[:, 0])).astype(np.int64)
+    # The same network on notes of the 64-job batch's preset (88 keys x 4 layers, stereo,
+    # loops, lpf_2p + filter envelope + LFO), rendered alone in the same way.
+    from claysampler_b200 import workload as wl
+    kit_root = root / "batch_preset"
+    kit_root.mkdir(parents=True, exist_ok=True)
+    kit_sfz = wl.write_plain_batch_preset(kit_root, seed=args.seed)
+    kit = (kit_sfz, lifetime.preset_regions(kit_sfz, 4.0))
+    bf, bt, bspans, _ = lifetime.render_training_set(kit_root, seed=args.seed + 7, jobs=args.learned_preset_jobs,
+                                                     notes=64, batch_jobs=64, device=f"cuda:{local}", kits=[kit],
+                                                     velocities=(40, 120), name="batch")
+    bpred = net.predict(bf).cpu().numpy()
+    bplain = lifetime.envelope_estimate(bf)
+    baudible = np.exp(bt[:, 0]).round().astype(np.int64)
+    bres_net = lifetime.admission_reservation(bpred[:, 0], bplain[:, 0], margin)
+    bres_plain = np.ceil(np.exp(bplain[:, 0])).astype(np.int64)
+    batch_preset = {
+        "notes": int(len(bf)),
+        "mae_log_frames": {"network": float(np.abs(bpred[:, 0] - bt[:, 0]).mean()),
+                           "plain": float(np.abs(bplain[:, 0] - bt[:, 0]).mean())},
+        "mae_peak_db": {"network": float(np.abs(bpred[:, 1] - bt[:, 1]).mean()),
+                        "plain": float(np.abs(bplain[:, 1] - bt[:, 1]).mean())},
+        "reserved_frames": {"network": int(bres_net.sum()), "plain": int(bres_plain.sum()),
+                            "audible": int(baudible.sum()), "rendered_spans": int(bspans.sum())},
+        "reservation_cut": float(1 - bres_net.sum() / bres_plain.sum()),
+        "mispredict_rate": {"network": float(np.mean(baudible > bres_net)),
+                            "plain": float(np.mean(baudible > bres_plain))}}
     out = {"metric": "learned note lifetime / peak: held-out mean absolute error and lifetime reservation",
            "value": float(np.abs(predicted[:, 0] - truth[:, 0]).mean()), "unit": "|log audible frames| error",
            "higher_is_better": False,
@@ -532,6 +574,7 @@ def run_learned(args):
            "reservation_cut": float(1 - reserve_net.sum() / reserve_plain.sum()),
            "mispredict_rate": {"network": float(np.mean(audible > reserve_net)),
                                "plain": float(np.mean(audible > reserve_plain))},
+           "batch_preset": batch_preset,
            "train_notes": int(train.sum()), "test_notes": int(test.sum()), "epochs": args.learned_epochs,
            "loss_first_last": [history[0], history[-1]],
            "train_ms": train_ms, "train_samples_per_s": 1e3 * args.learned_epochs * int(train.sum()) / train_ms,

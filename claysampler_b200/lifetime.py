@@ -310,19 +310,49 @@ def _region_for(regions: list[Region], key: int, velocity: int) -> Region:
     raise ValueError(f"no region for key {key} velocity {velocity}")
 
 
-def write_training_jobs(root: Path, seed: int, jobs: int, notes: int, instruments: int = 4) -> list[TrainingJob]:
+def preset_regions(sfz: Path, sample_seconds: float) -> list[Region]:
+    """Regions of a generated plain-batch preset (workload.write_plain_batch_preset): its
+    <global> envelope and filter opcodes, each region's key, velocity range, cutoff,
+    filter-envelope depth, LFO depth and loop mode."""
+    glob, regions = {}, []
+    for line in Path(sfz).read_text().splitlines():
+        fields = dict(tok.split("=", 1) for tok in line.split()[1:] if "=" in tok)
+        if line.startswith("<global>"):
+            glob = fields
+        elif line.startswith("<region>"):
+            o = {**glob, **fields}
+            key = int(o["key"])
+            regions.append(Region(
+                lokey=key, hikey=key, lovel=int(o["lovel"]), hivel=int(o["hivel"]), center=key,
+                attack=float(o.get("ampeg_attack", 0)), hold=float(o.get("ampeg_hold", 0)),
+                decay=float(o.get("ampeg_decay", 0)), sustain=float(o.get("ampeg_sustain", 100)) / 100,
+                release=float(o.get("ampeg_release", 0)),
+                cutoff=float(o["cutoff"]) if "cutoff" in o else NO_FILTER_HZ,
+                fileg_depth=float(o.get("fileg_depth", 0)), fileg_decay=float(o.get("fileg_decay", 0)),
+                fileg_sustain=float(o.get("fileg_sustain", 100)) / 100,
+                lfo_depth=float(o.get("lfo1_cutoff", 0)), loop=o.get("loop_mode") == "loop_continuous",
+                sample_seconds=sample_seconds))
+    return regions
+
+
+def write_training_jobs(root: Path, seed: int, jobs: int, notes: int, instruments: int = 4,
+                        kits: list[tuple[Path, list[Region]]] | None = None, velocities: tuple[int, int] = (1, 127),
+                        name: str = "train") -> list[TrainingJob]:
     """`jobs` MIDI files of `notes` isolated notes each: every note starts after the previous
-    one's release has ended, so each stretch of a job's render is one single-note render."""
+    one's release has ended, so each stretch of a job's render is one single-note render.
+    The instruments are `kits` ((sfz, regions) pairs), else `instruments` random ones."""
     rng = np.random.default_rng(seed)
-    kits = [write_training_instrument(root, seed * 1000 + i, f"train{i}") for i in range(instruments)]
+    if kits is None:
+        kits = [write_training_instrument(root, seed * 1000 + i, f"train{i}") for i in range(instruments)]
     out = []
     for j in range(jobs):
-        sfz, regions = kits[j % instruments]
-        job = TrainingJob(sfz=sfz, midi=root / f"train_{j:05d}.mid")
+        sfz, regions = kits[j % len(kits)]
+        job = TrainingJob(sfz=sfz, midi=root / f"{name}_{j:05d}.mid")
         onset = 0.05
+        keys = sorted({k for r in regions for k in range(r.lokey, r.hikey + 1)})
         for _ in range(notes):
-            key = int(rng.integers(21, 109))
-            velocity = int(rng.integers(1, 128))
+            key = int(rng.choice(keys))
+            velocity = int(rng.integers(velocities[0], velocities[1] + 1))
             held = _log_uniform(rng, 0.05, 3.0)
             region = _region_for(regions, key, velocity)
             job.notes.append(Note(onset, held, key, velocity, region))
@@ -355,7 +385,8 @@ def note_windows(plan, count: int) -> np.ndarray | None:
 
 
 def render_training_set(root: Path, seed: int = 11, jobs: int = 512, notes: int = 64, batch_jobs: int = 128,
-                        device: str = "cuda:0", host=None, renderer=None, instruments: int = 4):
+                        device: str = "cuda:0", host=None, renderer=None, instruments: int = 4, kits=None,
+                        velocities: tuple[int, int] = (1, 127), name: str = "train"):
     """Features and targets of single-note renders made by the renderer (natural mode).
 
     Returns (features (n, 16), targets (n, 2), planned frames of each note's spans,
@@ -364,7 +395,7 @@ def render_training_set(root: Path, seed: int = 11, jobs: int = 512, notes: int 
     from .renderer import Renderer
     own_host, own_renderer = host is None, renderer is None
     host = host or Host()
-    specs = write_training_jobs(root, seed, jobs, notes, instruments)
+    specs = write_training_jobs(root, seed, jobs, notes, instruments, kits, velocities, name)
     plans, kept, job_of = [], [], []
     for index, spec in enumerate(specs):
         plan = host.plan(spec.sfz, spec.midi, tail="natural")
