@@ -409,7 +409,8 @@ def run_b200(args):
                             "algorithmic_bytes": algorithmic[dominant], "traffic": traffic},
                "e2e": {"value": total_e2e_audio / max_e2e, "unit": "audio-s/s", "h2d_bytes_per_step": int(h2d),
                        "d2h_bytes_per_step": int(box.get("pcm", 0)), "ms_per_step": max_e2e * 1e3,
-                       "batch_jobs": e2e_batch, "autotune": tuned},
+                       "batch_jobs": e2e_batch, "autotune": tuned,
+                       "pass_ms": [round(t * 1e3, 2) for t in e2e_times]},
                "gpu_launches": launches, "clocks": clocks.summary()}
         if world == 1:
             try:

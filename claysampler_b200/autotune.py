@@ -7,9 +7,10 @@ end-to-end rate is how the job list is cut into GPU batches (`batch_jobs`, the
 CLI's --gpu-batch-jobs): larger batches launch fewer, larger grids, while smaller
 ones let the renderer's two stream lanes overlap one batch's upload and download
 with the other's kernels.  The best cut depends on the workload's lengths and on
-its voice mix, so :func:`tune` measures it.  It renders the workload through
-render_window for every candidate, one untimed pass, then the mean of `repeats`
-timed passes, and keeps the fastest.  Results are cached per workload signature in
+its voice mix, so :func:`tune` measures it.  After one discarded warm-up, it
+renders the workload through render_window for every candidate, one untimed pass
+and then `repeats` timed passes, and keeps the candidate whose median pass is
+fastest.  Results are cached per workload signature in
 a JSON file.  Candidates change only the batching, never the audio: publish
 order and PCM are the same for every cut (the renderer's invariant, tested in
 tests/test_serving.py).
@@ -54,12 +55,12 @@ def measure(plans, bank, batch_jobs: int, repeats: int = 2, device: int = 0) -> 
             start = time.perf_counter()
             renderer.render_window(plans, publish, copy=False)
             times.append(time.perf_counter() - start)
-        return audio[0] / (sum(times) / len(times))
+        return audio[0] / float(np.median(times))           # the median pass: host jitter aside
     finally:
         renderer.close()
 
 
-def tune(plans, bank, candidates=CANDIDATES, repeats: int = 2, device: int = 0,
+def tune(plans, bank, candidates=CANDIDATES, repeats: int = 3, device: int = 0,
          cache: Path | None = None) -> dict:
     """The fastest GPU batch size for `plans` ({"batch_jobs", "sweep", "signature"})."""
     key = signature(plans)
@@ -68,6 +69,7 @@ def tune(plans, bank, candidates=CANDIDATES, repeats: int = 2, device: int = 0,
         store = json.loads(cache.read_text())
         if key in store:
             return store[key]
+    measure(plans, bank, candidates[0], 1, device)        # one-time costs (threads, page-locking) land here
     sweep = {}
     for jobs in candidates:
         if jobs > 2 * len(plans) and sweep:
