@@ -216,6 +216,29 @@ def algorithmic_bytes(plans):
     return {"source": src, "recurrence": rec, "mix": mix}
 
 
+def sinc_flops(plans):
+    """FP32 flops of the 48-tap sinc MACs per launch of each stage: 2 * 48 * channels per
+    voice-frame of a span whose step is not 1 (at step 1 every position is a whole
+    frame and the MAC loop does not run), counted where the span is rendered (chains
+    in the source stage, the rest inline in the mix)."""
+    src = mix = 0.0
+    for p in plans:
+        s = p.spans
+        frames = (s["end"].astype(np.int64) - s["begin"]).astype(np.float64)
+        ch = s["channels"].astype(np.float64)
+        sinc = (s["step"] != 1.0) | (s["pitchSlope"] != 0) | (s["variablePitch"] != 0)
+        chain = s["filterTrack"] >= 0
+        flops = np.where(sinc, frames * ch * 96.0, 0.0)
+        src += float(np.sum(flops[chain]))
+        mix += float(np.sum(flops[~chain]))
+    return {"source": src, "mix": mix}
+
+
+def simt_fp32_tflops(sm_mhz):
+    """FP32 FMA peak of the 148 SMs (128 lanes each, 2 flops per FMA) at `sm_mhz`."""
+    return 2 * 128 * 148 * sm_mhz * 1e6 / 1e12
+
+
 def measured_peaks():
     path = ROOT / "MEASURED_PEAKS.json"
     if path.exists():
@@ -396,6 +419,16 @@ def run_b200(args):
         per_unit = traffic_per_unit()
         voice_frames = sum(p.voice_frames() for p in plans)
         traffic = per_unit[dominant] * voice_frames if dominant in per_unit else None
+        flops = sinc_flops(plans)
+        clock = clocks.summary().get("sm_mhz") or 1965.0
+        fp32_peak = simt_fp32_tflops(clock)
+        sinc_stage = "mix" if flops["mix"] >= flops["source"] else "source"
+        fp32 = None
+        if flops[sinc_stage] > 0 and stage_ms.get(sinc_stage):
+            rate = flops[sinc_stage] / (stage_ms[sinc_stage] * 1e-3) / 1e12
+            fp32 = {"kernel": sinc_stage, "achieved": rate, "peak": fp32_peak, "unit": "TFLOP/s",
+                    "frac": rate / fp32_peak, "flops": flops[sinc_stage],
+                    "peak_kind": f"SIMT FP32 FMA peak at the sampled {clock:.0f} MHz"}
         out = {"metric": METRIC, "value": total_audio / (max_ms * 1e-3), "unit": "audio-s/s", "n_gpus": world,
                "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SFZ/WAV/MIDI)",
@@ -406,7 +439,8 @@ def run_b200(args):
                "stage_ms": stage_ms,
                "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
                             "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                            "algorithmic_bytes": algorithmic[dominant], "traffic": traffic},
+                            "algorithmic_bytes": algorithmic[dominant], "traffic": traffic,
+                            "fp32_sinc": fp32},
                "e2e": {"value": total_e2e_audio / max_e2e, "unit": "audio-s/s", "h2d_bytes_per_step": int(h2d),
                        "d2h_bytes_per_step": int(box.get("pcm", 0)), "ms_per_step": max_e2e * 1e3,
                        "batch_jobs": e2e_batch, "autotune": tuned,
