@@ -104,9 +104,26 @@ __device__ __forceinline__ float2 sourceFrame(const float* __restrict__ bank, co
     return make_float2(left, v.channels == 1 ? left : __ldg(bank + index + 1));
 }
 
+// Eight consecutive weights of a sinc row: one 256-bit load (sm_100), so a warp's
+// request brings each lane a whole 32-byte sector of its own row.  `p` is 32-byte
+// aligned: rows are 192 bytes and the table starts on a 256-byte boundary.
+struct Weights8 {
+    float w[8];
+};
+
+__device__ __forceinline__ Weights8 sincWeights8(const float* p)
+{
+    Weights8 r;
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(r.w[0]), "=f"(r.w[1]), "=f"(r.w[2]), "=f"(r.w[3]), "=f"(r.w[4]), "=f"(r.w[5]), "=f"(r.w[6]),
+          "=f"(r.w[7])
+        : "l"(p));
+    return r;
+}
+
 // 48-tap windowed-sinc value at `pos` (render.cu:30-61).  The table is stored
 // phase-major, 48 contiguous weights per phase, so each lane streams its row with
-// 128-bit loads; the tap order of the accumulation is unchanged.
+// 256-bit loads; the tap order of the accumulation is unchanged.
 __device__ __forceinline__ float2 sincAt(const float* __restrict__ bank, const float* __restrict__ sinc,
                                          const cs_voice_span& v, double pos)
 {
@@ -115,32 +132,30 @@ __device__ __forceinline__ float2 sincAt(const float* __restrict__ bank, const f
         return sourceFrame(bank, v, center);
     const int phase = __double2int_rn((pos - double(center)) * kPhases);
     const float4* row = reinterpret_cast<const float4*>(sinc + size_t(phase) * kTaps);
+    const float* row1 = sinc + size_t(phase) * kTaps;
     float x = 0.f, y = 0.f;
     if (center >= 23 && center < v.sourceEnd - 24) {
         const float* s = bank + v.sample + uint64_t(center - 23) * uint64_t(v.channels);
         if (v.channels == 1) {
             #pragma unroll
-            for (int q = 0; q < kTaps / 4; ++q) {
-                const float4 w = __ldg(row + q);
-                x = fmaf(w.x, __ldg(s + 4 * q + 0), x);
-                x = fmaf(w.y, __ldg(s + 4 * q + 1), x);
-                x = fmaf(w.z, __ldg(s + 4 * q + 2), x);
-                x = fmaf(w.w, __ldg(s + 4 * q + 3), x);
+            for (int q = 0; q < kTaps / 8; ++q) {
+                const Weights8 w = sincWeights8(row1 + 8 * q);
+                #pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    x = fmaf(w.w[k], __ldg(s + 8 * q + k), x);
             }
             y = x;
         } else if ((reinterpret_cast<uintptr_t>(s) & 7) == 0) {
             const float2* s2 = reinterpret_cast<const float2*>(s);
             #pragma unroll
-            for (int q = 0; q < kTaps / 4; ++q) {
-                const float4 w = __ldg(row + q);
-                const float2 p0 = __ldg(s2 + 4 * q + 0);
-                const float2 p1 = __ldg(s2 + 4 * q + 1);
-                const float2 p2 = __ldg(s2 + 4 * q + 2);
-                const float2 p3 = __ldg(s2 + 4 * q + 3);
-                x = fmaf(w.x, p0.x, x); y = fmaf(w.x, p0.y, y);
-                x = fmaf(w.y, p1.x, x); y = fmaf(w.y, p1.y, y);
-                x = fmaf(w.z, p2.x, x); y = fmaf(w.z, p2.y, y);
-                x = fmaf(w.w, p3.x, x); y = fmaf(w.w, p3.y, y);
+            for (int q = 0; q < kTaps / 8; ++q) {
+                const Weights8 w = sincWeights8(row1 + 8 * q);
+                #pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const float2 pk = __ldg(s2 + 8 * q + k);
+                    x = fmaf(w.w[k], pk.x, x);
+                    y = fmaf(w.w[k], pk.y, y);
+                }
             }
         } else {
             // A stereo sample that starts at an odd float offset (after an odd-length
