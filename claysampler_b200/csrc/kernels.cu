@@ -815,8 +815,8 @@ __global__ void __launch_bounds__(kMixThreads, Inline ? 5 : 8) mixKernel(BatchVi
                 wetLeft += x * gains.x;
                 wetRight += x * gains.y;
             } else if (Inline) {
-                const float2 sample = voiceFrame(b.bank, b.sinc, b.voices[m.index], b.points, b.modulation, pan,
-                                                 frame, false, -1.0);
+                const float2 sample = voiceFrame<true>(b.bank, b.sinc, b.voices[m.index], b.points, b.modulation,
+                                                       pan, frame, false, -1.0);
                 left += sample.x;
                 right += sample.y;
             }

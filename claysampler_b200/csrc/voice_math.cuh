@@ -124,6 +124,7 @@ __device__ __forceinline__ Weights8 sincWeights8(const float* p)
 // 48-tap windowed-sinc value at `pos` (render.cu:30-61).  The table is stored
 // phase-major, 48 contiguous weights per phase, so each lane streams its row with
 // 256-bit loads; the tap order of the accumulation is unchanged.
+template <bool VectorTaps = false>
 __device__ __forceinline__ float2 sincAt(const float* __restrict__ bank, const float* __restrict__ sinc,
                                          const cs_voice_span& v, double pos)
 {
@@ -136,7 +137,32 @@ __device__ __forceinline__ float2 sincAt(const float* __restrict__ bank, const f
     float x = 0.f, y = 0.f;
     if (center >= 23 && center < v.sourceEnd - 24) {
         const float* s = bank + v.sample + uint64_t(center - 23) * uint64_t(v.channels);
-        if (v.channels == 1) {
+        const uint64_t first = v.sample + uint64_t(center - 23);     // float index of tap 0 (mono)
+        const uint64_t base = first & ~uint64_t(3);
+        if (VectorTaps && v.channels == 1 && base + 52 <= v.sample + uint64_t(v.sourceEnd)) {
+            // The 48 taps from thirteen aligned 128-bit loads of the 52 floats around
+            // them (all inside this sample), picked by the offset `first - base`
+            // (VectorTaps: for kernels with the registers to hold them).
+            const float4* s4 = reinterpret_cast<const float4*>(bank + base);
+            const int offset = int(first - base);
+            const bool odd = (offset & 1) != 0, two = (offset & 2) != 0;
+            float4 lo = __ldg(s4);
+            #pragma unroll
+            for (int q = 0; q < kTaps / 8; ++q) {
+                const Weights8 w = sincWeights8(row1 + 8 * q);
+                const float4 mid = __ldg(s4 + 2 * q + 1), hi = __ldg(s4 + 2 * q + 2);
+                const float f[12] = {lo.x, lo.y, lo.z, lo.w, mid.x, mid.y, mid.z, mid.w, hi.x, hi.y, hi.z, hi.w};
+                float g[10];
+                #pragma unroll
+                for (int i = 0; i < 10; ++i)
+                    g[i] = odd ? f[i + 1] : f[i];
+                #pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    x = fmaf(w.w[k], two ? g[k + 2] : g[k], x);
+                lo = hi;
+            }
+            y = x;
+        } else if (v.channels == 1) {
             #pragma unroll
             for (int q = 0; q < kTaps / 8; ++q) {
                 const Weights8 w = sincWeights8(row1 + 8 * q);
@@ -202,6 +228,7 @@ __device__ __forceinline__ double loopRemainder(double x, int period)
 // Source value of a voice at output `frame` (render.cu:63-100): position from the
 // span's start (or a precomputed variable-pitch phase), generators, loop wrap and
 // loop crossfade.
+template <bool VectorTaps = false>
 __device__ __forceinline__ float2 voiceSource(const float* __restrict__ bank, const float* __restrict__ sinc,
                                               const cs_voice_span& v, int frame, double pos)
 {
@@ -230,10 +257,10 @@ __device__ __forceinline__ float2 voiceSource(const float* __restrict__ bank, co
         pos = v.loopFirst + loopRemainder(pos - v.loopFirst, period);
     if (pos >= v.sourceEnd)
         return make_float2(0.f, 0.f);
-    float2 sample = sincAt(bank, sinc, v, pos);
+    float2 sample = sincAt<VectorTaps>(bank, sinc, v, pos);
     const int fadeStart = v.loopEnd - v.loopCrossfade;
     if (v.loopEnd > 0 && v.loopCrossfade > 0 && pos >= fadeStart) {
-        const float2 entry = sincAt(bank, sinc, v, pos - period);
+        const float2 entry = sincAt<VectorTaps>(bank, sinc, v, pos - period);
         const float phase = float((pos - fadeStart) / v.loopCrossfade);
         const float blend = .5f - .5f * cosf(3.14159265358979323846f * phase);
         sample.x = fmaf(blend, entry.x - sample.x, sample.x);
@@ -278,6 +305,7 @@ __device__ __forceinline__ void addVoiceMod(VoiceMods& s, int target, float valu
 // The voice frame from its modulation sums (render.cu:160-187).  With
 // `filterInput`, mono sources are returned before panning (the mix pans them after
 // the filter).
+template <bool VectorTaps = false>
 __device__ __forceinline__ float2 voiceOutput(const float* __restrict__ bank, const float* __restrict__ sinc,
                                               const cs_voice_span& v, const VoiceMods& s, int frame,
                                               bool filterInput, double phase)
@@ -285,7 +313,7 @@ __device__ __forceinline__ float2 voiceOutput(const float* __restrict__ bank, co
     float level = s.level;
     if (s.db != 0)
         level *= exp2f(s.db * .166096404744368f);
-    const float2 sample = voiceSource(bank, sinc, v, frame, phase);
+    const float2 sample = voiceSource<VectorTaps>(bank, sinc, v, frame, phase);
     if (filterInput && v.channels == 1)
         return make_float2(sample.x * level, sample.x * level);
     const float2 gains = panGains(v, s.pan);
@@ -311,6 +339,7 @@ __device__ __forceinline__ float2 voiceOutput(const float* __restrict__ bank, co
 }
 
 // Enveloped, modulated, panned voice frame (render.cu:138-187).
+template <bool VectorTaps = false>
 __device__ __forceinline__ float2 voiceFrame(const float* __restrict__ bank, const float* __restrict__ sinc,
                                              const cs_voice_span& v, const cs_control_point* __restrict__ points,
                                              const cs_voice_modulation* __restrict__ modulation, float pan,
@@ -327,7 +356,7 @@ __device__ __forceinline__ float2 voiceFrame(const float* __restrict__ bank, con
             continue;
         addVoiceMod(s, m.target, bindingAt(m, points, frame));
     }
-    return voiceOutput(bank, sinc, v, s, frame, filterInput, phase);
+    return voiceOutput<VectorTaps>(bank, sinc, v, s, frame, filterInput, phase);
 }
 
 // ---- filters (render.cu:276-336) ------------------------------------------------
