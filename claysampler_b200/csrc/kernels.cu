@@ -1268,10 +1268,20 @@ int launchGeneralChains(const BatchView& b, const SegmentView& s, cudaStream_t s
     return 1;
 }
 
+// The inline mix kernels need about 33 KB of shared memory per SM (five CTAs); the
+// rest of the SM's 256 KB goes to L1, where the 393 KB sinc table competes for room.
+constexpr int kInlineMixCarveout = 20;
+
 void launchMix(const BatchView& b, const SegmentView& s, bool natural, StereoStats* stats, cudaStream_t stream)
 {
     if (!s.blockCount)
         return;
+    static bool configured = false;
+    if (b.inlineVoices && !configured) {
+        cudaFuncSetAttribute(mixKernel<true, true>, cudaFuncAttributePreferredSharedMemoryCarveout, kInlineMixCarveout);
+        cudaFuncSetAttribute(mixKernel<false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, kInlineMixCarveout);
+        configured = true;
+    }
     if (natural) {
         if (b.inlineVoices)
             mixKernel<true, true><<<s.blockCount, kMixThreads, 0, stream>>>(b, s, stats);
