@@ -17,6 +17,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <mutex>
 
 namespace cs {
 
@@ -1230,15 +1231,29 @@ void launchPitch(const BatchView& b, const SegmentView& s, cudaStream_t stream)
     pitchKernel<<<(s.pitchCount + 63) / 64, 64, 0, stream>>>(b, s);
 }
 
+// Kernel attributes belong to a device's context, so they are set once per device.
+// True the first time it is called for `slot` with the current device.
+static bool firstOnDevice(int slot)
+{
+    static std::mutex guard;
+    static unsigned long long done[64] = {};
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64)
+        return true;
+    std::lock_guard<std::mutex> lock(guard);
+    const unsigned long long bit = 1ull << slot;
+    if (done[device] & bit)
+        return false;
+    done[device] |= bit;
+    return true;
+}
+
 int launchSources(const BatchView& b, const SegmentView& s, cudaStream_t stream)
 {
     if (!s.sourceTileCount)
         return 0;
-    static bool configured = false;
-    if (!configured) {
+    if (firstOnDevice(0))
         cudaFuncSetAttribute(sourceKernel, cudaFuncAttributePreferredSharedMemoryCarveout, kOverlapCarveout);
-        configured = true;
-    }
     sourceKernel<<<s.sourceTileCount, kSourceThreads, 0, stream>>>(b, s);
     return 1;
 }
@@ -1249,11 +1264,9 @@ int launchRecurrences(const BatchView& b, const SegmentView& s, cudaStream_t str
         return 0;
     constexpr int chainsPerCta = kRecWarps * kRecChains;
     constexpr int bytes = chainsPerCta * kRecChainBytes;
-    static bool configured = false;
-    if (!configured) {
+    if (firstOnDevice(1)) {
         cudaFuncSetAttribute(recurrenceKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
         cudaFuncSetAttribute(recurrenceKernel, cudaFuncAttributePreferredSharedMemoryCarveout, kOverlapCarveout);
-        configured = true;
     }
     recurrenceKernel<<<(s.simpleCount + chainsPerCta - 1) / chainsPerCta, kRecThreads, bytes, stream>>>(
         b, s, b.error);
@@ -1276,11 +1289,9 @@ void launchMix(const BatchView& b, const SegmentView& s, bool natural, StereoSta
 {
     if (!s.blockCount)
         return;
-    static bool configured = false;
-    if (b.inlineVoices && !configured) {
+    if (b.inlineVoices && firstOnDevice(2)) {
         cudaFuncSetAttribute(mixKernel<true, true>, cudaFuncAttributePreferredSharedMemoryCarveout, kInlineMixCarveout);
         cudaFuncSetAttribute(mixKernel<false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, kInlineMixCarveout);
-        configured = true;
     }
     if (natural) {
         if (b.inlineVoices)

@@ -187,3 +187,24 @@ def test_gpu_trained_network_beats_the_plain_estimate(tmp_path):
     assert err_net[0] < err_plain[0] and err_net[1] < err_plain[1], (err_net, err_plain)
     # the same predictions from the oracle
     np.testing.assert_allclose(predicted, ref.forward(*net.state(), features[test]), atol=2e-3)
+
+
+def test_preset_regions_and_reservation_rules(tmp_path):
+    """A generated batch preset's regions parse with its <global> defaults, and a
+    lifetime reservation never exceeds the plain bound and grows with the margin."""
+    from claysampler_b200 import lifetime, workload
+    sfz = workload.write_plain_batch_preset(tmp_path, seed=4, keys=range(60, 64), layers=2)
+    regions = lifetime.preset_regions(sfz, 4.0)
+    assert len(regions) == 8
+    assert all(r.attack == 0.005 and r.decay == 1.5 and r.sustain == 0.5 and r.release == 0.5 for r in regions)
+    assert all(200 <= r.cutoff <= 8000 and abs(r.fileg_depth) == 2400 for r in regions)
+    assert {r.loop for r in regions} == {True, False}
+    rng = np.random.default_rng(5)
+    truth = rng.normal(10, 1, 1000)
+    predicted = truth + rng.normal(0, 0.2, 1000)
+    margin = lifetime.calibrate_margin(predicted, truth, 0.01)
+    assert np.mean(truth - predicted > margin) <= 0.011
+    plain = truth + 0.5
+    reserved = lifetime.admission_reservation(predicted, plain, margin)
+    assert np.all(reserved <= np.ceil(np.exp(plain))) and np.all(reserved >= 1)
+    assert np.all(lifetime.admission_reservation(predicted, plain, margin + 0.1) >= reserved)
