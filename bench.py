@@ -1,33 +1,37 @@
 """Throughput of the batch voice-render path: audio-seconds rendered per second.
 
-Workload (default): the 64-job plain batch — one preset of 88 keys x 4 velocity
-layers of stereo 24-bit samples (half looping), lpf_2p with a +-2400 cent filter
-envelope and a 5 Hz LFO on the cutoff, MIDI lengths log-uniform 10-180 s at
-Poisson 4 notes/s with sustain-pedal toggles — generated from a seed (the
-reference's sample libraries are not redistributable) and planned by this
-package's C++ host.
+Workload (default, `--workload uneven`): the batching configuration — 1024 jobs
+over four presets of 12 mono 16-bit regions (keys up to four semitones from each
+keycenter, so most voices run the 48-tap sinc resampler), no filter, Pareto(1.5)
+lengths from 2 to 600 s — generated from a seed (the reference's sample libraries
+and MIDI corpora are not redistributable) and planned by this package's C++ host.
+`--workload plain_batch` renders instead the 64-job filtered batch: one preset of
+88 keys x 4 velocity layers of stereo 24-bit samples (half looping), lpf_2p with a
++-2400 cent filter envelope and a 5 Hz LFO on the cutoff, MIDI lengths
+log-uniform 10-180 s at Poisson 4 notes/s with sustain-pedal toggles.
 
 A step renders the whole batch: synthesis (sources, filter recurrences, mix) and
 natural-tail finishing to packed mono PCM16.  `value` times steps on inputs that
-are already resident in device memory (bank 497 MB and per-step scratch well
-above the 126 MB L2, so no flush is needed); `e2e` times the public
-render_window call with the plans in host memory, including the plan upload and
-the PCM download, in GPU batches (the CLI's --gpu-batch-jobs) whose size the
-autotuner (claysampler_b200/autotune.py) measured fastest for the workload, so
-that two batches in flight overlap their transfers with each other's kernels.
-Under torchrun every rank renders its own batch (no collective), so scaling is
-weak.
+are already resident in device memory (each step writes a float mix of gigabytes,
+well above the 126 MB L2, which evicts it between steps, so no flush is needed);
+`e2e` times the public render_window call with the plans in host memory,
+including the plan upload and the PCM download, in GPU batches (the CLI's
+--gpu-batch-jobs) whose size the autotuner (claysampler_b200/autotune.py)
+measured fastest for the workload.  Under torchrun every rank renders its own
+batch (no collective), so scaling is weak.
 
-`--workload uneven` renders instead the 1024-job batch of Pareto(1.5) lengths
-(four presets of the small mono kind, 48-tap sinc resampling on most voices).
-`--learned` trains and scores the note-lifetime predictor.
+`cpu_baseline` and `parity` (one rank): the first jobs of the workload planned by
+the reference's own planner and rendered by the reference's render.cu built for
+the host (oracle/_ref, all cores) with the oracle's tail.cu restatement; the GPU
+renders the same reference plans, and `parity` compares the two.
 
-`--serve` measures instead the submit-to-publish latency of requests that arrive
-one at a time (Poisson) through the non-blocking submit / poll pair.
+`--learned` trains and scores the note-lifetime predictor.  `--serve` measures
+the submit-to-publish latency of requests that arrive one at a time (Poisson)
+through the non-blocking submit / poll pair.
 
 `--impl reference` times the reference's own CPU implementation of the path
-(its src/cuda/render.cu built for the host, see oracle/ref) on a bounded sample
-of the same workload.
+(its planner and src/cuda/render.cu built for the host, see oracle/ref) on a
+bounded sample of the same workload, with the same `config`.
 """
 from __future__ import annotations
 
@@ -55,6 +59,9 @@ WORKLOADS = {
     "uneven": "uneven batch: 1024 jobs over 4 presets of 12 mono 16-bit regions (48-tap sinc resampling, "
               "no filter), Pareto(1.5) lengths 2-600 s",
 }
+# Jobs of the bounded CPU sample (the reference arm's step and the cpu_baseline /
+# parity leg): about 1-6 s of the reference's host render on 16 cores.
+CPU_SAMPLE_JOBS = {"plain_batch": 16, "uneven": 128}
 
 
 def parse():
@@ -63,11 +70,13 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    p.add_argument("--workload", choices=sorted(WORKLOADS), default="plain_batch",
-                   help="plain_batch: the 64-job filtered batch; uneven: 1024 Pareto-length jobs")
+    p.add_argument("--workload", choices=sorted(WORKLOADS), default="uneven",
+                   help="uneven: 1024 Pareto-length jobs (the batching configuration); plain_batch: the 64-job "
+                        "filtered batch")
     p.add_argument("--jobs", type=int, default=None, help="jobs per rank (default 64, or 1024 for uneven)")
     p.add_argument("--seed", type=int, default=2)
-    p.add_argument("--cpu-sample-jobs", type=int, default=32)
+    p.add_argument("--cpu-sample-jobs", type=int, default=None,
+                   help="jobs of the bounded CPU sample (default: 128 for uneven, 16 for plain_batch)")
     p.add_argument("--workdir", type=Path, default=Path(tempfile.gettempdir()) / "claysampler_bench")
     p.add_argument("--e2e-batch-jobs", type=int, default=32,
                    help="GPU batch size of the end-to-end pass (the CLI's --gpu-batch-jobs): two batches in "
@@ -262,26 +271,85 @@ def traffic_per_unit():
     return table
 
 
-def cpu_baseline(plans, bank, sample_jobs):
-    """The reference's render.cu built for the host (oracle/_ref), all cores, on the
-    first `sample_jobs` jobs; the oracle restatement when that build is absent."""
-    from oracle import oracle
-    sample = plans[:sample_jobs]
+def sample_jobs(args):
+    """The bounded CPU sample: the first jobs of the workload (jobs are drawn
+    independently, so a prefix is an unbiased sample of the lengths)."""
+    if args.cpu_sample_jobs is None:
+        args.cpu_sample_jobs = CPU_SAMPLE_JOBS.get(args.workload, 32)
+    return args.cpu_sample_jobs
+
+
+def bench_config(args, jobs, ranks):
+    """The `config` object of the bench line, identical in both arms."""
+    return {"workload": WORKLOADS[args.workload], "jobs_per_gpu": len(jobs), "seed": args.seed, "tail": "natural",
+            "taps": 48, "l2": "each step writes a float mix above the 126 MB L2, evicting it (no flush)",
+            "parallelism": f"jobs sharded by rank, {ranks} rank(s)"}
+
+
+def reference_render(jobs, threads):
+    """The reference end to end on the host: its own planner (oracle/_ref, the
+    reference's plan.cpp / instrument.cpp / midi.cpp / audio.cpp) plans `jobs`, its
+    render.cu built for the host renders them on `threads` cores and the oracle's
+    restatement of tail.cu finishes them.  Returns (plans, bank, render) where
+    render() times one pass and returns (seconds, pcm, results, mix)."""
+    from oracle import oracle, reference
+    if not reference.available():
+        reference.build()
+    if not reference.available():
+        raise RuntimeError("the reference is not built for the host (oracle/_ref)")
+    session = reference.RefSession()
+    plans = [session.plan(sfz, midi, tail="natural") for sfz, midi in jobs]
+    bank = session.bank()
+    session.close()
+
+    def render():
+        start = time.perf_counter()
+        mix = reference.synthesize(plans, bank, True, threads)
+        pcm, results = oracle.finish(mix, plans)
+        return time.perf_counter() - start, pcm, results, mix
+    return plans, bank, render
+
+
+def cpu_baseline(jobs, sample_jobs, host_plans, host_bank, renderer):
+    """The reference on the host cores (its planner and its render.cu built for the
+    host, all cores) over the first `sample_jobs` jobs, and the parity of this
+    package on the same jobs: its planner's plans byte for byte against the
+    reference planner's, and the GPU render of the reference's plans against the
+    reference's render (float bus error in full scale, PCM16 LSBs, statuses and
+    frames)."""
     threads = os.cpu_count() or 1
-    try:
-        from oracle import reference
-        if not reference.available():
-            raise RuntimeError
-        synth, kind = reference.synthesize, "reference"
-    except Exception:
-        synth, kind = oracle.synthesize, "port"
-    start = time.perf_counter()
-    mix = synth(sample, bank, True, threads)
-    _, results = oracle.finish(mix, sample)
-    seconds = time.perf_counter() - start
+    sample = jobs[:sample_jobs]
+    plans, bank, render = reference_render(sample, threads)
+    seconds, pcm, results, mix = render()
     audio = float(results["frames"].sum()) / RATE
-    return {"value": audio / seconds, "unit": "audio-s/s", "cores": threads, "kind": kind,
-            "sample": f"first {len(sample)} of {len(plans)} jobs ({audio:.1f} output audio-s), natural tail"}
+    baseline = {"value": audio / seconds, "unit": "audio-s/s", "cores": threads, "kind": "reference",
+                "sample": f"first {len(sample)} of {len(jobs)} jobs ({audio:.1f} output audio-s), natural tail, "
+                          "planned by the reference planner"}
+    prepared = renderer.prepare(plans)
+    try:
+        prepared.run()
+        gpu_pcm, gpu_results = prepared.collect()
+        gpu_mix = prepared.mix()
+    finally:
+        prepared.close()
+    diff = np.abs(gpu_pcm.astype(np.int32) - pcm.astype(np.int32)) if gpu_pcm.shape == pcm.shape else None
+    same_plans = all(a.to_blob() == b.to_blob() for a, b in zip(host_plans[:len(plans)], plans))
+    # The renderer holds this package's bank; the reference plans index the
+    # reference's, which must be the same floats.
+    same_plans = same_plans and bank.size <= host_bank.size and np.array_equal(bank, host_bank[:bank.size])
+    parity = {"jobs": len(plans), "plans_identical": bool(same_plans),  # plans and sample bank
+              "max_bus_error_fs": float(np.max(np.abs(gpu_mix - mix))) if gpu_mix.shape == mix.shape else None,
+              "max_lsb": int(diff.max()) if diff is not None and diff.size else (0 if diff is not None else None),
+              "identical_fraction": float(np.mean(diff == 0)) if diff is not None and diff.size else None,
+              "statuses_equal": bool(np.array_equal(gpu_results["status"], results["status"])),
+              "frames_equal": bool(np.array_equal(gpu_results["frames"], results["frames"])),
+              "against": "the reference's planner + render.cu on the host + the oracle's tail.cu restatement",
+              "bounds": "bus <= 1e-5 FS, PCM16 <= 1 LSB with >= 99.9 % identical, statuses and frames exact"}
+    parity["ok"] = bool(parity["plans_identical"] and parity["statuses_equal"] and parity["frames_equal"]
+                        and parity["max_bus_error_fs"] is not None and parity["max_bus_error_fs"] <= 1e-5
+                        and parity["max_lsb"] is not None and parity["max_lsb"] <= 1
+                        and (parity["identical_fraction"] or 1.0) >= 0.999)
+    return baseline, parity
 
 
 def run_reference(args):
@@ -289,24 +357,16 @@ def run_reference(args):
     if rank != 0:
         return
     jobs = workload(args, 0)
-    plans, bank = plan_jobs(jobs)
-    sample = plans[:args.cpu_sample_jobs]
+    sample = jobs[:sample_jobs(args)]
+    threads = os.cpu_count() or 1
     try:
-        from oracle import oracle, reference
-        if not reference.available():
-            reference.build()
-        kind = "reference" if reference.available() else "port"
-        synth = reference.synthesize if kind == "reference" else oracle.synthesize
-    except Exception as error:  # no host build of the reference and no restatement
+        plans, bank, render = reference_render(sample, threads)
+    except Exception as error:  # no host build of the reference
         print(json.dumps({"impl": "reference", "unavailable": f"reference CPU path unavailable: {error}"}))
         return
-    threads = os.cpu_count() or 1
     times, audio = [], 0.0
     for i in range(args.warmup + args.steps):
-        start = time.perf_counter()
-        mix = synth(sample, bank, True, threads)
-        _, results = oracle.finish(mix, sample)
-        elapsed = time.perf_counter() - start
+        elapsed, _, results, _ = render()
         audio = float(results["frames"].sum()) / RATE
         if i >= args.warmup:
             times.append(elapsed)
@@ -315,10 +375,10 @@ def run_reference(args):
     out = {"metric": METRIC, "value": value, "unit": "audio-s/s", "n_gpus": args.gpus, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SFZ/WAV/MIDI)", "impl": "reference",
-           "config": {"workload": WORKLOADS[args.workload], "sample": f"first {len(sample)} jobs",
-                      "tail": "natural"},
-           "cpu_baseline": {"value": value, "unit": "audio-s/s", "cores": threads, "kind": kind,
-                            "sample": f"first {len(sample)} of {len(plans)} jobs per step"},
+           "config": bench_config(args, jobs, args.gpus),
+           "cpu_baseline": {"value": value, "unit": "audio-s/s", "cores": threads, "kind": "reference",
+                            "sample": f"first {len(sample)} of {len(jobs)} jobs per step ({audio:.1f} output "
+                                      "audio-s), planned by the reference planner"},
            "e2e": {"value": value, "unit": "audio-s/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
 
@@ -422,25 +482,25 @@ def run_b200(args):
         flops = sinc_flops(plans)
         clock = clocks.summary().get("sm_mhz") or 1965.0
         fp32_peak = simt_fp32_tflops(clock)
-        sinc_stage = "mix" if flops["mix"] >= flops["source"] else "source"
         fp32 = None
-        if flops[sinc_stage] > 0 and stage_ms.get(sinc_stage):
-            rate = flops[sinc_stage] / (stage_ms[sinc_stage] * 1e-3) / 1e12
-            fp32 = {"kernel": sinc_stage, "achieved": rate, "peak": fp32_peak, "unit": "TFLOP/s",
-                    "frac": rate / fp32_peak, "flops": flops[sinc_stage],
+        if flops.get(dominant, 0.0) > 0 and stage_ms.get(dominant):
+            rate = flops[dominant] / (stage_ms[dominant] * 1e-3) / 1e12
+            fp32 = {"kernel": dominant, "achieved": rate, "peak": fp32_peak, "unit": "TFLOP/s",
+                    "frac": rate / fp32_peak, "flops": flops[dominant],
                     "peak_kind": f"SIMT FP32 FMA peak at the sampled {clock:.0f} MHz"}
+        roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                    "unit": "GB/s", "frac": achieved / peak, "algorithmic_bytes": algorithmic[dominant],
+                    "traffic": traffic, "fp32_sinc": fp32}
+        # The binding roof of the dominant kernel is the one it is closest to.
+        roofline["binding"] = "fp32" if fp32 and fp32["frac"] > roofline["frac"] else "hbm"
+        bank_mb = float(bank.nbytes) / 1e6
         out = {"metric": METRIC, "value": total_audio / (max_ms * 1e-3), "unit": "audio-s/s", "n_gpus": world,
                "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SFZ/WAV/MIDI)",
-               "config": {"workload": WORKLOADS[args.workload], "jobs_per_gpu": len(plans), "seed": args.seed,
-                          "output_audio_s_per_gpu": audio, "voice_frames_per_gpu": voice_frames,
-                          "tail": "natural", "taps": 48, "l2": "inputs larger than L2 (no flush)",
-                          "parallelism": f"jobs sharded by rank, {world} rank(s)", "statuses": statuses},
-               "stage_ms": stage_ms,
-               "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
-                            "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                            "algorithmic_bytes": algorithmic[dominant], "traffic": traffic,
-                            "fp32_sinc": fp32},
+               "config": bench_config(args, jobs, world),
+               "workload_stats": {"output_audio_s_per_gpu": audio, "voice_frames_per_gpu": voice_frames,
+                                  "bank_mb": bank_mb, "statuses": statuses},
+               "stage_ms": stage_ms, "roofline": roofline,
                "e2e": {"value": total_e2e_audio / max_e2e, "unit": "audio-s/s", "h2d_bytes_per_step": int(h2d),
                        "d2h_bytes_per_step": int(box.get("pcm", 0)), "ms_per_step": max_e2e * 1e3,
                        "batch_jobs": e2e_batch, "autotune": tuned,
@@ -448,7 +508,7 @@ def run_b200(args):
                "gpu_launches": launches, "clocks": clocks.summary()}
         if world == 1:
             try:
-                out["cpu_baseline"] = cpu_baseline(plans, bank, args.cpu_sample_jobs)
+                out["cpu_baseline"], out["parity"] = cpu_baseline(jobs, sample_jobs(args), plans, bank, renderer)
             except Exception as error:
                 out["cpu_baseline"] = {"value": None, "unavailable": str(error)}
         print(json.dumps(out))

@@ -17,6 +17,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <initializer_list>
 #include <mutex>
 
 namespace cs {
@@ -1231,29 +1232,43 @@ void launchPitch(const BatchView& b, const SegmentView& s, cudaStream_t stream)
     pitchKernel<<<(s.pitchCount + 63) / 64, 64, 0, stream>>>(b, s);
 }
 
-// Kernel attributes belong to a device's context, so they are set once per device.
-// True the first time it is called for `slot` with the current device.
-static bool firstOnDevice(int slot)
+// Kernel attributes belong to a device's context, so they are set once per device:
+// `set` runs under the lock the first time `slot` is seen on the current device,
+// and the slot is marked done only when every attribute call succeeded (a failed
+// set is retried by the next launch; no launch proceeds before the set returns).
+template <class Set>
+static void setOncePerDevice(int slot, Set&& set)
 {
     static std::mutex guard;
     static unsigned long long done[64] = {};
     int device = 0;
-    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64)
-        return true;
+    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) {
+        set();
+        return;
+    }
     std::lock_guard<std::mutex> lock(guard);
     const unsigned long long bit = 1ull << slot;
     if (done[device] & bit)
-        return false;
-    done[device] |= bit;
-    return true;
+        return;
+    if (set() == cudaSuccess)
+        done[device] |= bit;
+}
+
+static cudaError_t firstError(std::initializer_list<cudaError_t> statuses)
+{
+    for (const cudaError_t s : statuses)
+        if (s != cudaSuccess)
+            return s;
+    return cudaSuccess;
 }
 
 int launchSources(const BatchView& b, const SegmentView& s, cudaStream_t stream)
 {
     if (!s.sourceTileCount)
         return 0;
-    if (firstOnDevice(0))
-        cudaFuncSetAttribute(sourceKernel, cudaFuncAttributePreferredSharedMemoryCarveout, kOverlapCarveout);
+    setOncePerDevice(0, [] {
+        return cudaFuncSetAttribute(sourceKernel, cudaFuncAttributePreferredSharedMemoryCarveout, kOverlapCarveout);
+    });
     sourceKernel<<<s.sourceTileCount, kSourceThreads, 0, stream>>>(b, s);
     return 1;
 }
@@ -1264,10 +1279,11 @@ int launchRecurrences(const BatchView& b, const SegmentView& s, cudaStream_t str
         return 0;
     constexpr int chainsPerCta = kRecWarps * kRecChains;
     constexpr int bytes = chainsPerCta * kRecChainBytes;
-    if (firstOnDevice(1)) {
-        cudaFuncSetAttribute(recurrenceKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        cudaFuncSetAttribute(recurrenceKernel, cudaFuncAttributePreferredSharedMemoryCarveout, kOverlapCarveout);
-    }
+    setOncePerDevice(1, [] {
+        return firstError({cudaFuncSetAttribute(recurrenceKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+                           cudaFuncSetAttribute(recurrenceKernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                                kOverlapCarveout)});
+    });
     recurrenceKernel<<<(s.simpleCount + chainsPerCta - 1) / chainsPerCta, kRecThreads, bytes, stream>>>(
         b, s, b.error);
     return 1;
@@ -1289,10 +1305,13 @@ void launchMix(const BatchView& b, const SegmentView& s, bool natural, StereoSta
 {
     if (!s.blockCount)
         return;
-    if (b.inlineVoices && firstOnDevice(2)) {
-        cudaFuncSetAttribute(mixKernel<true, true>, cudaFuncAttributePreferredSharedMemoryCarveout, kInlineMixCarveout);
-        cudaFuncSetAttribute(mixKernel<false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, kInlineMixCarveout);
-    }
+    if (b.inlineVoices)
+        setOncePerDevice(2, [] {
+            return firstError({cudaFuncSetAttribute(mixKernel<true, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                                    kInlineMixCarveout),
+                               cudaFuncSetAttribute(mixKernel<false, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                                    kInlineMixCarveout)});
+        });
     if (natural) {
         if (b.inlineVoices)
             mixKernel<true, true><<<s.blockCount, kMixThreads, 0, stream>>>(b, s, stats);

@@ -9,8 +9,9 @@
 // of fixed size instead of the renderer's arena.  Its limit is
 // CS_STATIC_FINISH_MAX_FRAMES frames and CS_STATIC_FINISH_MAX_JOBS jobs per call.
 // Every call reuses the same array and leaves the last call's contents in it;
-// every word a call reads is written earlier in the same call, so nothing needs
-// clearing.  Calls whose work overlaps on the GPU (on different streams, or from
+// every word a call reads is written earlier in the same call (the job tables by
+// a set-up kernel from the job records, which the launch carries as its
+// parameter), so nothing needs clearing.  Calls whose work overlaps on the GPU (on different streams, or from
 // different threads) race on the array and must be serialised by the caller.
 #include "kernels.cuh"
 
@@ -18,7 +19,6 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
-#include <vector>
 
 namespace cs {
 namespace {
@@ -64,6 +64,70 @@ unsigned char* scratchOnCurrentDevice()
 
 thread_local std::string lastStaticError;
 
+// The job table travels to the device as a kernel parameter (4 KB of records
+// copied into the launch itself), so the call stages nothing through pageable
+// memory and reads no host memory after it returns.
+struct FinishTable {
+    cs_finish_job jobs[kMaxJobs];
+    int count, window;
+};
+static_assert(sizeof(FinishTable) <= 32764, "kernel parameter limit");
+
+// One CTA of kMaxJobs threads: thread j owns job j.  Exclusive scans of the jobs'
+// frames, 1024-frame blocks and tail windows give each job's offsets; then the
+// CTA writes the job of every block and window (a binary search over the scanned
+// offsets in shared memory).
+__global__ void __launch_bounds__(kMaxJobs) finishSetupKernel(FinishTable t, JobInfo* jobs, int* blockJob,
+                                                              int* windowJob)
+{
+    __shared__ unsigned long long frameBase[kMaxJobs];
+    __shared__ int blockBase[kMaxJobs + 1], windowBase[kMaxJobs + 1];
+    const int j = int(threadIdx.x);
+    const int frames = j < t.count ? t.jobs[j].frames : 0;
+    const int blocks = (frames + kBlockFrames - 1) / kBlockFrames;
+    const int windows = (frames + t.window - 1) / t.window;
+    frameBase[j] = (unsigned long long)frames;
+    blockBase[j + 1] = blocks;
+    windowBase[j + 1] = windows;
+    if (j == 0)
+        blockBase[0] = windowBase[0] = 0;
+    __syncthreads();
+    // Inclusive scans (Hillis-Steele); frameBase is made exclusive afterwards.
+    for (int d = 1; d < kMaxJobs; d <<= 1) {
+        const unsigned long long f = j >= d ? frameBase[j - d] : 0ull;
+        const int b = j >= d ? blockBase[j + 1 - d] : 0, w = j >= d ? windowBase[j + 1 - d] : 0;
+        __syncthreads();
+        frameBase[j] += f;
+        blockBase[j + 1] += b;
+        windowBase[j + 1] += w;
+        __syncthreads();
+    }
+    if (j < t.count) {
+        JobInfo info{};
+        info.offset = frameBase[j] - (unsigned long long)frames;
+        info.frames = frames;
+        info.musicEnd = t.jobs[j].music_end;
+        info.limit = t.jobs[j].limit;
+        info.fade = t.jobs[j].fade_frames;
+        info.blockFirst = blockBase[j];
+        info.windowFirst = windowBase[j];
+        jobs[j] = info;
+    }
+    const auto owner = [](const int* base, int count, int item) {
+        int low = 0, high = count;                 // base[low] <= item < base[high]
+        while (low + 1 < high) {
+            const int mid = (low + high) >> 1;
+            if (base[mid] <= item) low = mid;
+            else high = mid;
+        }
+        return low;
+    };
+    for (int b = j; b < blockBase[t.count]; b += kMaxJobs)
+        blockJob[b] = owner(blockBase, t.count, b);
+    for (int w = j; w < windowBase[t.count]; w += kMaxJobs)
+        windowJob[w] = owner(windowBase, t.count, w);
+}
+
 } // namespace
 } // namespace cs
 
@@ -79,44 +143,28 @@ extern "C" int cs_finish_natural_static(const float* mix, const cs_finish_job* j
                                         std::to_string(kMaxJobs));
         if (rate <= 0 || window < int(kMinWindow))
             throw std::invalid_argument("cs_finish_natural_static: invalid rate or window");
-        std::vector<JobInfo> info(static_cast<size_t>(count));
-        std::vector<int> blockJob, windowJob;
+        FinishTable table;
+        table.count = count;
+        table.window = window;
         size_t frames = 0;
         int blocks = 0, windows = 0;
         for (int j = 0; j < count; ++j) {
             const cs_finish_job& job = jobs[j];
             if (job.frames <= 0)
                 throw std::invalid_argument("cs_finish_natural_static: job " + std::to_string(j) + " has no frames");
-            JobInfo& out = info[size_t(j)];
-            out = {};
-            out.offset = frames;
-            out.frames = job.frames;
-            out.musicEnd = job.music_end;
-            out.limit = job.limit;
-            out.fade = job.fade_frames;
-            out.blockFirst = blocks;
-            out.windowFirst = windows;
+            table.jobs[j] = job;
             frames += size_t(job.frames);
             if (frames > kMaxFrames)
                 throw std::invalid_argument("cs_finish_natural_static: the jobs' " + std::to_string(frames) +
                                             "+ frames exceed the limit of " + std::to_string(kMaxFrames));
-            const int jobBlocks = (job.frames + kBlockFrames - 1) / kBlockFrames;
-            const int jobWindows = (job.frames + window - 1) / window;
-            blockJob.insert(blockJob.end(), size_t(jobBlocks), j);
-            windowJob.insert(windowJob.end(), size_t(jobWindows), j);
-            blocks += jobBlocks;
-            windows += jobWindows;
+            blocks += (job.frames + kBlockFrames - 1) / kBlockFrames;
+            windows += (job.frames + window - 1) / window;
         }
         unsigned char* scratch = scratchOnCurrentDevice();
         const auto s = static_cast<cudaStream_t>(stream);
-        const auto put = [&](size_t at, const void* data, size_t bytes) {
-            const cudaError_t status = cudaMemcpyAsync(scratch + at, data, bytes, cudaMemcpyHostToDevice, s);
-            if (status != cudaSuccess)
-                throw std::runtime_error(std::string("static finishing upload: ") + cudaGetErrorString(status));
-        };
-        put(kJobsAt, info.data(), info.size() * sizeof(JobInfo));
-        put(kBlockJobAt, blockJob.data(), blockJob.size() * sizeof(int));
-        put(kWindowJobAt, windowJob.data(), windowJob.size() * sizeof(int));
+        finishSetupKernel<<<1, kMaxJobs, 0, s>>>(table, reinterpret_cast<JobInfo*>(scratch + kJobsAt),
+                                                  reinterpret_cast<int*>(scratch + kBlockJobAt),
+                                                  reinterpret_cast<int*>(scratch + kWindowJobAt));
 
         BatchView view{};
         view.jobs = reinterpret_cast<const JobInfo*>(scratch + kJobsAt);

@@ -271,8 +271,13 @@ int cs_renderer_set_scratch_limit(cs_renderer* renderer, size_t bytes);
  * CS_STATIC_FINISH_MAX_FRAMES frames and CS_STATIC_FINISH_MAX_JOBS jobs (larger
  * calls fail with a message from cs_finish_natural_static_error); window >= 400.
  * The first call on each device looks up the array's device address with that
- * device current, so make it before any stream capture.  All calls share the
- * array: calls whose work overlaps on the GPU race and must be serialised.
+ * device current; with CUDA's lazy module loading (the default) that first
+ * lookup also loads the library's device code and places the array, which can
+ * allocate and synchronise, so make the first call at set-up time, outside the
+ * real-time path and before any stream capture.  Later calls allocate nothing:
+ * the job records travel to the device inside a set-up kernel's launch
+ * parameters (no pageable host-to-device copy).  All calls share the array:
+ * calls whose work overlaps on the GPU race and must be serialised.
  * `packed` receives up to the sum of frames int16 samples and `results` one
  * cs_tail_result per job, exactly as the renderer's natural finishing writes
  * them.  Enqueued on `stream` (a cudaStream_t; NULL = the legacy default stream);

@@ -51,17 +51,26 @@ def test_static_finishing_matches_renderer(plain_small, batch_mini):
     jobs = (FinishJob * len(plans))(*[FinishJob(p.frames, p.music_end, p.limit, p.fade_frames) for p in plans])
     frames = sum(p.frames for p in plans)
     mix_d = torch.from_numpy(mix).cuda()
+    # Both calls' outputs are allocated up front, so that device memory can be
+    # compared across the second call: after the first call on a device (which
+    # loads the module holding the static array), a call allocates nothing.
+    packed_d = [torch.full((frames,), 12345, dtype=torch.int16, device="cuda") for _ in range(2)]
+    results_d = [torch.zeros(len(plans) * TAIL_RESULT.itemsize, dtype=torch.uint8, device="cuda") for _ in range(2)]
+    free_before = None
     for call in range(2):
-        packed_d = torch.full((frames,), 12345, dtype=torch.int16, device="cuda")
-        results_d = torch.zeros(len(plans) * TAIL_RESULT.itemsize, dtype=torch.uint8, device="cuda")
-        status = lib.cs_finish_natural_static(mix_d.data_ptr(), jobs, len(plans), 44100, 2205, packed_d.data_ptr(),
-                                              results_d.data_ptr(), None)
+        torch.cuda.synchronize()
+        if call == 1:
+            free_before = torch.cuda.mem_get_info()[0]
+        status = lib.cs_finish_natural_static(mix_d.data_ptr(), jobs, len(plans), 44100, 2205,
+                                              packed_d[call].data_ptr(), results_d[call].data_ptr(), None)
         assert status == 0, lib.cs_finish_natural_static_error().decode()
         torch.cuda.synchronize()
-        results = np.frombuffer(results_d.cpu().numpy().tobytes(), TAIL_RESULT)
+        if call == 1:
+            assert torch.cuda.mem_get_info()[0] == free_before, "the second call changed free device memory"
+        results = np.frombuffer(results_d[call].cpu().numpy().tobytes(), TAIL_RESULT)
         for field in ("status", "frames", "dataFrames", "fade", "offset", "peak", "first", "last"):
             np.testing.assert_array_equal(results[field], expected[field], err_msg=f"call {call}: {field}")
-        pcm = packed_d.cpu().numpy()[:expected_pcm.size]
+        pcm = packed_d[call].cpu().numpy()[:expected_pcm.size]
         assert int(np.max(np.abs(pcm.astype(np.int32) - expected_pcm.astype(np.int32)))) <= 1, f"call {call}"
 
 
