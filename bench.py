@@ -36,6 +36,7 @@ bounded sample of the same workload, with the same `config`.
 from __future__ import annotations
 
 import argparse
+import contextlib
 import json
 import os
 import statistics
@@ -400,38 +401,52 @@ def run_b200(args):
         plan.pin()
     renderer = Renderer(device=local, natural=True, batch_jobs=len(plans))
     renderer.upload_samples(bank)
-    prepared = renderer.prepare(plans)
-    prepared.set_profile(True)
     stream = torch.cuda.Stream()          # a real stream: handle 0 would mean the renderer's own
 
     def barrier():
         if distributed:
             torch.distributed.barrier()
 
-    for _ in range(args.warmup):
-        prepared.run(stream.cuda_stream)
-    torch.cuda.synchronize()
+    def timed(prepared, clocks=None):
+        """Warm-up steps, then `steps` steps each bracketed by CUDA events on the
+        launching stream; per-stage device times summed over the steps."""
+        for _ in range(args.warmup):
+            prepared.run(stream.cuda_stream)
+        torch.cuda.synchronize()
+        totals, step_ms = {}, []
+        with (clocks or contextlib.nullcontext()):
+            barrier()
+            torch.cuda.synchronize()
+            for _ in range(args.steps):
+                start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                start.record(stream)
+                prepared.run(stream.cuda_stream)
+                end.record(stream)
+                end.synchronize()
+                step_ms.append(start.elapsed_time(end))
+                for name, stage in prepared.stage_ms().items():
+                    totals[name] = totals.get(name, 0.0) + stage
+            barrier()
+            torch.cuda.synchronize()
+        return sum(step_ms) / len(step_ms), totals
+
+    # The plain path first: every voice frame resampled inline.
+    renderer.set_shared_sources(False)
+    plain = renderer.prepare(plans)
+    plain.set_profile(True)
+    plain_ms, plain_totals = timed(plain)
+    plain.close()
+    # The batched form: each voice source shared by several voices of the batch
+    # rendered once (bit-identical audio).
+    renderer.set_shared_sources(True)
+    prepared = renderer.prepare(plans)
+    prepared.set_profile(True)
+    shared_info = prepared.shared
+    clocks = ClockSampler(local)
+    ms, stage_totals = timed(prepared, clocks)
     _, results = prepared.collect()
     audio = float(results["frames"].sum()) / RATE
     statuses = np.bincount(results["status"], minlength=12).tolist()
-
-    stage_totals = {}
-    with ClockSampler(local) as clocks:
-        barrier()
-        torch.cuda.synchronize()
-        step_ms = []
-        for _ in range(args.steps):
-            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            start.record(stream)
-            prepared.run(stream.cuda_stream)
-            end.record(stream)
-            end.synchronize()
-            step_ms.append(start.elapsed_time(end))
-            for name, ms in prepared.stage_ms().items():
-                stage_totals[name] = stage_totals.get(name, 0.0) + ms
-        barrier()
-        torch.cuda.synchronize()
-    ms = sum(step_ms) / len(step_ms)
     launches = prepared.launches * args.steps
 
     # End to end through the public API: plans in host memory, PCM back to host, in
@@ -472,14 +487,19 @@ def run_b200(args):
     if rank == 0:
         peak, peak_kind = measured_peaks()
         algorithmic = algorithmic_bytes(plans)
+        flops = sinc_flops(plans)
+        # Shared voice sources: their sinc MACs move from the mix to the shared
+        # stage, which reads each source's samples once and writes it once.
+        flops["mix"] -= 96.0 * shared_info["voice_sinc_floats"]
+        flops["shared"] = 96.0 * shared_info["sinc_floats"]
+        algorithmic["shared"] = 8.0 * shared_info["floats"]
         stage_ms = {k: v / args.steps for k, v in stage_totals.items()}
-        candidates = {k: stage_ms.get(k, 0.0) for k in ("source", "recurrence", "mix")}
+        candidates = {k: stage_ms.get(k, 0.0) for k in ("source", "recurrence", "mix", "shared")}
         dominant = max(candidates, key=candidates.get)
         achieved = algorithmic[dominant] / (stage_ms[dominant] * 1e-3) / 1e9
         per_unit = traffic_per_unit()
         voice_frames = sum(p.voice_frames() for p in plans)
         traffic = per_unit[dominant] * voice_frames if dominant in per_unit else None
-        flops = sinc_flops(plans)
         clock = clocks.summary().get("sm_mhz") or 1965.0
         fp32_peak = simt_fp32_tflops(clock)
         fp32 = None
@@ -493,6 +513,13 @@ def run_b200(args):
                     "traffic": traffic, "fp32_sinc": fp32}
         # The binding roof of the dominant kernel is the one it is closest to.
         roofline["binding"] = "fp32" if fp32 and fp32["frac"] > roofline["frac"] else "hbm"
+        # Every synthesis stage against both roofs.
+        roofline["stages"] = {
+            k: {"ms": stage_ms[k], "gbs": algorithmic.get(k, 0.0) / (stage_ms[k] * 1e-3) / 1e9,
+                "hbm_frac": algorithmic.get(k, 0.0) / (stage_ms[k] * 1e-3) / 1e9 / peak,
+                "sinc_tflops": flops.get(k, 0.0) / (stage_ms[k] * 1e-3) / 1e12,
+                "fp32_frac": flops.get(k, 0.0) / (stage_ms[k] * 1e-3) / 1e12 / fp32_peak}
+            for k in ("source", "recurrence", "mix", "shared") if stage_ms.get(k, 0.0) > 0.01}
         bank_mb = float(bank.nbytes) / 1e6
         out = {"metric": METRIC, "value": total_audio / (max_ms * 1e-3), "unit": "audio-s/s", "n_gpus": world,
                "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms, "higher_is_better": True,
@@ -501,6 +528,11 @@ def run_b200(args):
                "workload_stats": {"output_audio_s_per_gpu": audio, "voice_frames_per_gpu": voice_frames,
                                   "bank_mb": bank_mb, "statuses": statuses},
                "stage_ms": stage_ms, "roofline": roofline,
+               "plain": {"value": audio / (plain_ms * 1e-3), "ms_per_step": plain_ms,
+                         "stage_ms": {k: v / args.steps for k, v in plain_totals.items()},
+                         "what": "every voice frame resampled inline (shared voice sources off)"},
+               "batched_vs_plain": plain_ms / ms,
+               "shared_sources": shared_info,
                "e2e": {"value": total_e2e_audio / max_e2e, "unit": "audio-s/s", "h2d_bytes_per_step": int(h2d),
                        "d2h_bytes_per_step": int(box.get("pcm", 0)), "ms_per_step": max_e2e * 1e3,
                        "batch_jobs": e2e_batch, "autotune": tuned,

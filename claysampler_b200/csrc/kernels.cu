@@ -700,6 +700,31 @@ __global__ void __launch_bounds__(kRecThreads, 1) recurrenceKernel(BatchView b, 
     }
 }
 
+// ---- shared voice sources ------------------------------------------------------------
+//
+// One CTA per 256-frame tile of a shared source, a thread per frame: the voice
+// source of render.cu:63-100 (position, loop wrap and crossfade, 48-tap sinc) at
+// the elapsed frame, stored as one float (mono) or two (stereo).  The mix then
+// reads it for every voice that plays the source.
+__global__ void __launch_bounds__(kSourceThreads) sharedSourceKernel(BatchView b, const SharedSource* __restrict__ sources,
+                                                                     const int2* __restrict__ tiles)
+{
+    const int2 tile = tiles[blockIdx.x];
+    const SharedSource source = sources[tile.x];
+    const cs_voice_span& v = b.voices[source.voice];
+    const int end = min(source.frames, tile.y + kSourceTile);
+    float* out = b.shared + source.offset;
+    const bool stereo = v.channels == 2;
+    #pragma unroll 1
+    for (int i = tile.y + int(threadIdx.x); i < end; i += kSourceThreads) {
+        const float2 x = voiceSource<true>(b.bank, b.sinc, v, v.begin + i, -1.0);
+        if (stereo)
+            reinterpret_cast<float2*>(out)[i] = x;
+        else
+            out[i] = x.x;
+    }
+}
+
 // ---- mix + block scan ----------------------------------------------------------------
 
 constexpr int kMixThreads = 256;
@@ -731,9 +756,38 @@ struct MinOp { __device__ int operator()(int a, int b) const { return a < b ? a 
 // A tile's voice as the mix reads it: frame range, where its filtered frames
 // start (in floats, relative to frame 0 of the job), its index and kind.
 struct MixVoice {
-    long long offset;                   // filtered + offset + frame * channels is the frame's first sample
-    int begin, end, index, kind;        // kind: 0 unfiltered, 1 filtered stereo, 2 filtered mono
+    long long offset;                   // filtered (shared) + offset + frame * channels is the frame's first sample
+    int begin, end, index, kind;        // kind: 0 unfiltered, 1 filtered stereo, 2 filtered mono,
+                                        // 3 shared mono source, 4 shared stereo source
+    int sharedEnd;                      // kinds 3, 4: frames from here on have a silent source
 };
+
+// A tile's voice as the mix reads it (the staged and unstaged paths alike).
+__device__ __forceinline__ MixVoice mixVoiceOf(const BatchView& b, const SegmentView& s, int index)
+{
+    const cs_voice_span& v = b.voices[index];
+    MixVoice m;
+    m.begin = v.begin;
+    m.end = v.end;
+    m.index = index;
+    m.sharedEnd = 0;
+    if (v.filterTrack >= 0) {
+        m.kind = v.channels == 1 ? 2 : 1;
+        m.offset = (long long)s.scratchOffset[index] - (long long)max(v.begin, s.first) * v.channels;
+    } else {
+        m.kind = 0;
+        m.offset = 0;
+        if (b.sharedRefs) {
+            const SharedRef ref = b.sharedRefs[index];
+            if (ref.offset >= 0) {
+                m.kind = v.channels == 1 ? 3 : 4;
+                m.offset = ref.offset - (long long)v.begin * v.channels;
+                m.sharedEnd = v.begin + ref.frames;
+            }
+        }
+    }
+    return m;
+}
 
 constexpr int kMixStaged = kMixThreads / kTilesPerBlock;     // staged voices per tile
 
@@ -768,19 +822,7 @@ __global__ void __launch_bounds__(kMixThreads, Inline ? 5 : 8) mixKernel(BatchVi
                 atomicOr(&mixedTiles, 1 << k);
         }
         if (i < tile.count && tile.count <= kMixStaged) {
-            const int index = __ldg(b.indices + tile.first + i);
-            const cs_voice_span& v = b.voices[index];
-            MixVoice m;
-            m.begin = v.begin;
-            m.end = v.end;
-            m.index = index;
-            if (v.filterTrack >= 0) {
-                m.kind = v.channels == 1 ? 2 : 1;
-                m.offset = (long long)s.scratchOffset[index] - (long long)max(v.begin, s.first) * v.channels;
-            } else {
-                m.kind = 0;
-                m.offset = 0;
-            }
+            const MixVoice m = mixVoiceOf(b, s, __ldg(b.indices + tile.first + i));
             if (m.kind != 1)
                 atomicOr(&mixedTiles, 1 << k);
             staged[k][i] = m;
@@ -816,11 +858,30 @@ __global__ void __launch_bounds__(kMixThreads, Inline ? 5 : 8) mixKernel(BatchVi
                 const float2 gains = panGains(v, offset);
                 wetLeft += x * gains.x;
                 wetRight += x * gains.y;
-            } else if (Inline) {
+            } else if (Inline && m.kind == 0) {
                 const float2 sample = voiceFrame<true>(b.bank, b.sinc, b.voices[m.index], b.points, b.modulation,
                                                        pan, frame, false, -1.0);
                 left += sample.x;
                 right += sample.y;
+            } else if (Inline) {
+                // voiceFrame with the source read from the shared sources.
+                const cs_voice_span& v = b.voices[m.index];
+                const float level = envelopeAt(v, frame);
+                if (level > 0) {
+                    const VoiceMods mods = voiceMods(v, b.points, b.modulation, level, pan, frame);
+                    float2 source = make_float2(0.f, 0.f);
+                    if (frame < m.sharedEnd) {
+                        if (m.kind == 3) {
+                            const float x = __ldg(b.shared + (m.offset + frame));
+                            source = make_float2(x, x);
+                        } else {
+                            source = __ldg(reinterpret_cast<const float2*>(b.shared + (m.offset + 2ll * frame)));
+                        }
+                    }
+                    const float2 sample = voiceOutputFrom(source, v, mods, false);
+                    left += sample.x;
+                    right += sample.y;
+                }
             }
         };
         if (!(mixedTiles >> k & 1)) {
@@ -850,18 +911,8 @@ __global__ void __launch_bounds__(kMixThreads, Inline ? 5 : 8) mixKernel(BatchVi
             for (int i = 0; i < tile.count; ++i)
                 addVoice(staged[k][i]);
         } else {
-            for (int i = tile.first; i < tile.first + tile.count; ++i) {
-                const int index = __ldg(b.indices + i);
-                const cs_voice_span& v = b.voices[index];
-                MixVoice m;
-                m.begin = v.begin;
-                m.end = v.end;
-                m.index = index;
-                m.kind = v.filterTrack < 0 ? 0 : v.channels == 1 ? 2 : 1;
-                m.offset = v.filterTrack < 0 ? 0
-                    : (long long)s.scratchOffset[index] - (long long)max(v.begin, s.first) * v.channels;
-                addVoice(m);
-            }
+            for (int i = tile.first; i < tile.first + tile.count; ++i)
+                addVoice(mixVoiceOf(b, s, __ldg(b.indices + i)));
         }
         const float amplitude = jobGainAt(b.points, job.tracks, frame);
         const float x = fmaf(left, amplitude, wetLeft), y = fmaf(right, amplitude, wetRight);
@@ -1223,6 +1274,15 @@ void launchScan(const BatchView& b, StereoStats* stats, int blocks, cudaStream_t
 {
     if (blocks)
         scanKernel<<<blocks, kMixThreads, 0, stream>>>(b, stats, blocks);
+}
+
+int launchSharedSources(const BatchView& b, const SharedSource* sources, const int2* tiles, int tileCount,
+                        cudaStream_t stream)
+{
+    if (!tileCount)
+        return 0;
+    sharedSourceKernel<<<tileCount, kSourceThreads, 0, stream>>>(b, sources, tiles);
+    return 1;
 }
 
 void launchPitch(const BatchView& b, const SegmentView& s, cudaStream_t stream)

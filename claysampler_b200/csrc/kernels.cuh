@@ -60,6 +60,23 @@ struct TailConfig {                     // src/cuda/render_types.h:100-103
     double relative, floor, ceiling;
 };
 
+// A voice source shared by the voices of a batch that play the same sample from
+// the same position at the same step, with the same loop and pitch ramp: their
+// resampled source (render.cu:63-100) depends only on the frames elapsed since the
+// voice began, so it is rendered once per batch and each voice reads it.
+struct SharedSource {
+    long long offset;                   // float offset of the source's frames in BatchView::shared
+    int voice;                          // a voice playing it (its span fields define the source)
+    int frames;                         // frames rendered; a voice's later frames are silent
+};
+
+// Per voice: where its shared source starts (-1: resampled inline) and how many
+// of its frames the shared source covers.
+struct SharedRef {
+    long long offset;
+    int frames, pad;
+};
+
 // Everything one synthesis pass reads, as device pointers.
 struct BatchView {
     const float* bank;
@@ -77,6 +94,8 @@ struct BatchView {
     double* phase;
     void* mix;                          // float2 (natural) or short2
     int* error;                         // set by kernels whose bounded waits ran out
+    float* shared;                      // shared voice sources (mono: 1 float per frame, stereo: 2)
+    const SharedRef* sharedRefs;        // per voice (null when no source is shared)
     int jobCount;
     int inlineVoices;                   // some voice has no filter chain (the mix renders it)
 };
@@ -169,6 +188,10 @@ void launchScan(const BatchView& b, StereoStats* stats, int blocks, cudaStream_t
 // (span, first frame, end frame, first tile).
 void launchExpandTiles(const int4* runs, int count, int2* tiles, cudaStream_t stream);
 void launchPitch(const BatchView& b, const SegmentView& s, cudaStream_t stream);
+// Renders the shared voice sources: `tiles` holds (source, first frame) every
+// kSourceTile frames.
+int launchSharedSources(const BatchView& b, const SharedSource* sources, const int2* tiles, int tileCount,
+                        cudaStream_t stream);
 int launchSources(const BatchView& b, const SegmentView& s, cudaStream_t stream);
 int launchRecurrences(const BatchView& b, const SegmentView& s, cudaStream_t stream);
 int launchGeneralChains(const BatchView& b, const SegmentView& s, cudaStream_t stream);

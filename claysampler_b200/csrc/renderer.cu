@@ -19,6 +19,8 @@
 #include <deque>
 #include <limits>
 #include <memory>
+#include <tuple>
+#include <map>
 #include <numeric>
 #include <stdexcept>
 #include <string>
@@ -529,6 +531,130 @@ SegmentTables planSegments(const HostBatch& batch, size_t budget)
     return t;
 }
 
+// Shared voice sources: voices rendered inline (no filter chain) that play the
+// same sample from the same position at the same step, with the same loop, loop
+// crossfade and pitch ramp, have the same resampled source at every elapsed frame
+// (render.cu:63-100 reads nothing else), so a batch renders it once and the mix
+// reads it for each of them.  The audio is unchanged: the source is the same
+// function of the same doubles.  Generators and variable-pitch voices stay inline.
+struct SharedPlan {
+    std::vector<SharedSource> sources;
+    std::vector<SharedRef> refs;        // per voice; empty when nothing is shared
+    std::vector<int4> runs;             // (source, 0, frames, first tile) for tile expansion
+    size_t tiles = 0, floats = 0;
+    long long sharedVoiceFrames = 0;    // voice frames that read a shared source
+    // Channel-frames that run the 48-tap sinc (step or pitch ramp away from 1):
+    // rendered in the shared sources, and of the voices that read them instead.
+    long long sincFloats = 0, sincVoiceFloats = 0;
+};
+
+bool resamples(const cs_voice_span& v) { return v.step != 1.0 || v.pitchSlope != 0; }
+
+// The first elapsed frame at which a voice without loop or pitch ramp is past
+// its sample's end, with the device's double arithmetic (position + elapsed x step,
+// multiplied and added separately); every later frame is past it as well.
+long long silentFrom(const cs_voice_span& v)
+{
+    const double span = double(v.sourceEnd) - v.position;
+    long long e = std::max<long long>(0, (long long)std::floor(span / v.step) - 2);
+    for (;;) {
+        const double distance = double(e);
+        const double product = distance * v.step;
+        const double pos = v.position + product;
+        if (pos >= double(v.sourceEnd))
+            return e;
+        ++e;
+    }
+}
+
+SharedPlan planSharedSources(const HostBatch& batch, size_t budgetBytes)
+{
+    struct Key {
+        uint64_t sample;
+        double position, step, slope;
+        int channels, sourceEnd, loopFirst, loopEnd, loopCrossfade;
+        bool operator<(const Key& o) const
+        {
+            return std::tie(sample, position, step, slope, channels, sourceEnd, loopFirst, loopEnd, loopCrossfade) <
+                std::tie(o.sample, o.position, o.step, o.slope, o.channels, o.sourceEnd, o.loopFirst, o.loopEnd,
+                         o.loopCrossfade);
+        }
+    };
+    struct Entry {
+        int voice = -1, frames = 0, users = 0;
+        long long total = 0;
+    };
+    SharedPlan plan;
+    const size_t count = batch.voices.size();
+    std::map<Key, Entry> entries;
+    std::vector<const Entry*> entryOf(count, nullptr);
+    for (size_t i = 0; i < count; ++i) {
+        const cs_voice_span& v = batch.voices[i];
+        if (v.filterTrack >= 0 || v.generator != CS_GEN_NONE || v.variablePitch || v.end <= v.begin ||
+            v.channels < 1 || v.channels > 2)
+            continue;
+        long long frames = v.end - v.begin;
+        if (v.loopEnd <= 0 && v.pitchSlope == 0 && v.step > 0)
+            frames = std::min(frames, silentFrom(v));
+        const Key key{v.sample, v.position, v.step, v.pitchSlope, v.channels, v.sourceEnd, v.loopFirst, v.loopEnd,
+                      v.loopCrossfade};
+        Entry& e = entries[key];
+        if (e.voice < 0)
+            e.voice = int(i);
+        e.frames = int(std::max<long long>(e.frames, frames));
+        e.users += 1;
+        e.total += frames;
+        entryOf[i] = &e;
+    }
+    // Sources played by more than one voice, the most voice frames saved first,
+    // within the budget.
+    std::vector<const Entry*> chosen;
+    for (const auto& kv : entries)
+        if (kv.second.users > 1 && kv.second.frames > 0)
+            chosen.push_back(&kv.second);
+    std::stable_sort(chosen.begin(), chosen.end(), [](const Entry* a, const Entry* b) {
+        return a->total - a->frames > b->total - b->frames;
+    });
+    std::map<const Entry*, long long> offsetOf;
+    size_t bytes = 0;
+    for (const Entry* e : chosen) {
+        const int channels = batch.voices[size_t(e->voice)].channels;
+        const size_t floats = alignFloats(size_t(e->frames) * size_t(channels));
+        if ((plan.floats + floats) * sizeof(float) > budgetBytes)
+            continue;
+        offsetOf[e] = (long long)plan.floats;
+        SharedSource source{};
+        source.offset = (long long)plan.floats;
+        source.voice = e->voice;
+        source.frames = e->frames;
+        plan.runs.push_back(make_int4(int(plan.sources.size()), 0, e->frames, int(plan.tiles)));
+        plan.tiles += size_t(e->frames + kSourceTile - 1) / kSourceTile;
+        plan.sources.push_back(source);
+        plan.floats += floats;
+        if (resamples(batch.voices[size_t(e->voice)]))
+            plan.sincFloats += (long long)e->frames * channels;
+        bytes += floats * sizeof(float);
+    }
+    if (plan.sources.empty())
+        return plan;
+    if (plan.tiles > size_t(INT32_MAX))
+        throw std::runtime_error("too many shared source tiles in one batch");
+    plan.refs.assign(count, SharedRef{-1, 0, 0});
+    for (size_t i = 0; i < count; ++i) {
+        if (!entryOf[i])
+            continue;
+        const auto at = offsetOf.find(entryOf[i]);
+        if (at == offsetOf.end())
+            continue;
+        plan.refs[i] = SharedRef{at->second, entryOf[i]->frames, 0};
+        const cs_voice_span& v = batch.voices[i];
+        plan.sharedVoiceFrames += v.end - v.begin;
+        if (resamples(v))
+            plan.sincVoiceFloats += (long long)(v.end - v.begin) * v.channels;
+    }
+    return plan;
+}
+
 } // namespace
 } // namespace cs
 
@@ -544,6 +670,9 @@ struct cs_prepared {
     int lane = 0;                       // the renderer lane whose streams run the batch
     cs::HostBatch batch;
     cs::SegmentTables tables;
+    cs::SharedPlan shared;              // shared voice sources (empty: every source inline)
+    const cs::SharedSource* sharedSources = nullptr;
+    const int2* sharedTiles = nullptr;
     void* arena = nullptr;
     size_t arenaBytes = 0;
     cs::BatchView view{};
@@ -594,6 +723,7 @@ struct cs_renderer {
     float* bank = nullptr;
     size_t bankCapacity = 0, uploaded = 0;
     size_t scratchLimit = 0;            // 0: derive from free memory
+    bool sharedSources = true;          // render each shared voice source once per batch
     size_t peak = 0, waiting = 0, peakWaiting = 0, spilled = 0, downloaded = 0, cacheBudget = 0;
     size_t live = 0;                    // bytes of prepared batches alive
     void* hostPcm = nullptr;
@@ -690,8 +820,12 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
             p->groups.push_back(make_int2(int(first), int(end)));
         }
     }
-    p->tables = planSegments(batch, r.scratchLimit ? r.scratchLimit : defaultScratchBudget());
+    const size_t scratchBudget = r.scratchLimit ? r.scratchLimit : defaultScratchBudget();
+    p->tables = planSegments(batch, scratchBudget);
     const SegmentTables& t = p->tables;
+    if (r.sharedSources)
+        p->shared = planSharedSources(batch, scratchBudget / 2);
+    const SharedPlan& sh = p->shared;
     const size_t jobs = batch.jobs.size();
     const size_t frameBytes = r.natural ? sizeof(float2) : sizeof(short2);
     const int channels = r.natural ? 1 : 2;
@@ -719,6 +853,9 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     const size_t oOnsets = section(batch.onsets.size() * sizeof(int));
     const size_t oOnsetJob = section(batch.onsetJob.size() * sizeof(int));
     const size_t oGroups = section(p->groups.size() * sizeof(int2));
+    const size_t oSharedSources = section(sh.sources.size() * sizeof(SharedSource));
+    const size_t oSharedRefs = section(sh.refs.size() * sizeof(SharedRef));
+    const size_t oSharedRuns = section(sh.runs.size() * sizeof(int4));
     const size_t uploadEnd = layout.bytes;
     p->stateBytes = batch.voices.size() * sizeof(ChainState);
     const size_t oStates = section(p->stateBytes);
@@ -731,6 +868,8 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     const size_t oMono = section(r.natural ? batch.frames * sizeof(short) : 0);
     const size_t oPacked = section(batch.frames * size_t(channels) * sizeof(short));
     const size_t oSourceTiles = section(t.tileCount * sizeof(int2));
+    const size_t oSharedTiles = section(sh.tiles * sizeof(int2));
+    const size_t oShared = section(sh.floats * sizeof(float));
     const size_t oScratch = section(t.scratchBytes);
     const size_t oError = section(sizeof(int));
     p->bodyBytes = size_t(batch.bodyWindows) * sizeof(unsigned long long);
@@ -809,6 +948,9 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     stage(oOnsets, batch.onsets);
     stage(oOnsetJob, batch.onsetJob);
     stage(oGroups, p->groups);
+    stage(oSharedSources, sh.sources);
+    stage(oSharedRefs, sh.refs);
+    stage(oSharedRuns, sh.runs);
     // Copy and upload the staged ranges in slices: each slice's DMA runs while the
     // workers copy the next slice.  Ranges are the staged pieces merged across small
     // gaps (section alignment); the direct uploads follow them in stream order, so
@@ -844,6 +986,8 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     // the device: millions of them for an hour of voices.
     launchExpandTiles(reinterpret_cast<const int4*>(base + oTileRuns), int(t.tileRuns.size()),
                       reinterpret_cast<int2*>(base + oSourceTiles), lane.stream);
+    launchExpandTiles(reinterpret_cast<const int4*>(base + oSharedRuns), int(sh.runs.size()),
+                      reinterpret_cast<int2*>(base + oSharedTiles), lane.stream);
     check(cudaGetLastError(), "CUDA source tile expansion");
     check(cudaStreamSynchronize(lane.stream), "CUDA batch upload");
 
@@ -862,6 +1006,10 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     v.filtered = reinterpret_cast<float*>(base + oScratch);
     v.mix = base + oMix;
     v.error = reinterpret_cast<int*>(base + oError);
+    v.shared = reinterpret_cast<float*>(base + oShared);
+    v.sharedRefs = sh.refs.empty() ? nullptr : reinterpret_cast<const SharedRef*>(base + oSharedRefs);
+    p->sharedSources = reinterpret_cast<const SharedSource*>(base + oSharedSources);
+    p->sharedTiles = reinterpret_cast<const int2*>(base + oSharedTiles);
     v.jobCount = int(jobs);
     v.inlineVoices = std::any_of(batch.voices.begin(), batch.voices.end(),
                                  [](const cs_voice_span& voice) { return voice.filterTrack < 0; }) ? 1 : 0;
@@ -931,8 +1079,8 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     return p.release();
 }
 
-const char* const kStageNames[] = {"pitch", "source", "recurrence", "general", "mix", "finish", "assess"};
-constexpr int kStages = 7;
+const char* const kStageNames[] = {"pitch", "source", "recurrence", "general", "mix", "finish", "assess", "shared"};
+constexpr int kStages = 8;
 
 void run(cs_renderer& r, cs_prepared& p, cudaStream_t stream)
 {
@@ -962,6 +1110,8 @@ void run(cs_renderer& r, cs_prepared& p, cudaStream_t stream)
     if (p.bodyBytes)
         check(cudaMemsetAsync(p.finish.bodyPower, 0, p.bodyBytes, stream), "CUDA body power reset");
     stage(-1);
+    launches += launchSharedSources(p.view, p.sharedSources, p.sharedTiles, int(p.shared.tiles), stream);
+    stage(7);
     for (size_t i = 0; i < p.segments.size(); ++i) {
         BatchView view = p.view;
         const SegmentPlan& plan = p.tables.segments[i];
@@ -1844,6 +1994,25 @@ int cs_renderer_set_scratch_limit(cs_renderer* r, size_t bytes)
             throw std::runtime_error("null renderer");
         r->scratchLimit = bytes;
     });
+}
+
+int cs_renderer_set_shared_sources(cs_renderer* r, int enable)
+{
+    return cs::guarded([&] {
+        if (!r)
+            throw std::runtime_error("null renderer");
+        r->sharedSources = enable != 0;
+    });
+}
+
+size_t cs_prepared_shared_sources(const cs_prepared* p) { return p ? p->shared.sources.size() : 0; }
+size_t cs_prepared_shared_frames(const cs_prepared* p) { return p ? p->shared.floats : 0; }
+long long cs_prepared_shared_voice_frames(const cs_prepared* p) { return p ? p->shared.sharedVoiceFrames : 0; }
+long long cs_prepared_shared_sinc(const cs_prepared* p, long long* voice_floats)
+{
+    if (voice_floats)
+        *voice_floats = p ? p->shared.sincVoiceFloats : 0;
+    return p ? p->shared.sincFloats : 0;
 }
 
 size_t cs_prepared_segments(const cs_prepared* p) { return p ? p->tables.segments.size() : 0; }

@@ -302,18 +302,15 @@ __device__ __forceinline__ void addVoiceMod(VoiceMods& s, int target, float valu
     }
 }
 
-// The voice frame from its modulation sums (render.cu:160-187).  With
-// `filterInput`, mono sources are returned before panning (the mix pans them after
-// the filter).
-template <bool VectorTaps = false>
-__device__ __forceinline__ float2 voiceOutput(const float* __restrict__ bank, const float* __restrict__ sinc,
-                                              const cs_voice_span& v, const VoiceMods& s, int frame,
-                                              bool filterInput, double phase)
+// The voice frame from its modulation sums and its source value `sample`
+// (render.cu:160-187).  With `filterInput`, mono sources are returned before
+// panning (the mix pans them after the filter).
+__device__ __forceinline__ float2 voiceOutputFrom(float2 sample, const cs_voice_span& v, const VoiceMods& s,
+                                                  bool filterInput)
 {
     float level = s.level;
     if (s.db != 0)
         level *= exp2f(s.db * .166096404744368f);
-    const float2 sample = voiceSource<VectorTaps>(bank, sinc, v, frame, phase);
     if (filterInput && v.channels == 1)
         return make_float2(sample.x * level, sample.x * level);
     const float2 gains = panGains(v, s.pan);
@@ -338,6 +335,32 @@ __device__ __forceinline__ float2 voiceOutput(const float* __restrict__ bank, co
     return make_float2(l * level, r * level);
 }
 
+// The voice frame from its modulation sums, resampling its source at `frame`.
+template <bool VectorTaps = false>
+__device__ __forceinline__ float2 voiceOutput(const float* __restrict__ bank, const float* __restrict__ sinc,
+                                              const cs_voice_span& v, const VoiceMods& s, int frame,
+                                              bool filterInput, double phase)
+{
+    return voiceOutputFrom(voiceSource<VectorTaps>(bank, sinc, v, frame, phase), v, s, filterInput);
+}
+
+// Modulation sums of one voice frame over its voice-level bindings, in binding
+// order (render.cu:138-160); `level` is the enveloped level.
+__device__ __forceinline__ VoiceMods voiceMods(const cs_voice_span& v, const cs_control_point* __restrict__ points,
+                                               const cs_voice_modulation* __restrict__ modulation, float level,
+                                               float pan, int frame)
+{
+    VoiceMods s{level, 0.f, pan, 0.f, 0.f};
+    const int modEnd = v.firstModulation + v.modulationCount;
+    for (int j = v.firstModulation; j < modEnd; ++j) {
+        const cs_voice_modulation m = modulation[j];
+        if (m.target > CS_MOD_POSITION)
+            continue;
+        addVoiceMod(s, m.target, bindingAt(m, points, frame));
+    }
+    return s;
+}
+
 // Enveloped, modulated, panned voice frame (render.cu:138-187).
 template <bool VectorTaps = false>
 __device__ __forceinline__ float2 voiceFrame(const float* __restrict__ bank, const float* __restrict__ sinc,
@@ -348,14 +371,7 @@ __device__ __forceinline__ float2 voiceFrame(const float* __restrict__ bank, con
     const float level = envelopeAt(v, frame);
     if (level <= 0)
         return make_float2(0.f, 0.f);
-    VoiceMods s{level, 0.f, pan, 0.f, 0.f};
-    const int modEnd = v.firstModulation + v.modulationCount;
-    for (int j = v.firstModulation; j < modEnd; ++j) {
-        const cs_voice_modulation m = modulation[j];
-        if (m.target > CS_MOD_POSITION)
-            continue;
-        addVoiceMod(s, m.target, bindingAt(m, points, frame));
-    }
+    const VoiceMods s = voiceMods(v, points, modulation, level, pan, frame);
     return voiceOutput<VectorTaps>(bank, sinc, v, s, frame, filterInput, phase);
 }
 

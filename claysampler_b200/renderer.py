@@ -55,6 +55,14 @@ def library() -> ctypes.CDLL:
         lib.cs_prepared_segments.restype = sz
         lib.cs_prepared_destroy.argtypes = [vp]
         lib.cs_renderer_set_scratch_limit.argtypes = [vp, sz]
+        lib.cs_renderer_set_shared_sources.argtypes = [vp, i32]
+        for name in ("cs_prepared_shared_sources", "cs_prepared_shared_frames"):
+            getattr(lib, name).argtypes = [vp]
+            getattr(lib, name).restype = sz
+        lib.cs_prepared_shared_voice_frames.argtypes = [vp]
+        lib.cs_prepared_shared_voice_frames.restype = c.c_longlong
+        lib.cs_prepared_shared_sinc.argtypes = [vp, c.POINTER(c.c_longlong)]
+        lib.cs_prepared_shared_sinc.restype = c.c_longlong
         lib.cs_submit.argtypes = [vp, vp, sz, c.POINTER(c.c_uint64)]
         lib.cs_poll.argtypes = [vp, i32, vp, vp, c.POINTER(sz)]
         lib.cs_pending_jobs.argtypes = [vp]
@@ -140,13 +148,25 @@ class Prepared:
     def segments(self) -> int:
         return library().cs_prepared_segments(self.handle)
 
+    @property
+    def shared(self) -> dict:
+        """Shared voice sources of the batch: how many, the floats they hold and
+        the voice frames that read them instead of resampling."""
+        lib = library()
+        voice_sinc = ctypes.c_longlong()
+        sinc = lib.cs_prepared_shared_sinc(self.handle, ctypes.byref(voice_sinc))
+        return {"sources": int(lib.cs_prepared_shared_sources(self.handle)),
+                "floats": int(lib.cs_prepared_shared_frames(self.handle)),
+                "voice_frames": int(lib.cs_prepared_shared_voice_frames(self.handle)),
+                "sinc_floats": int(sinc), "voice_sinc_floats": int(voice_sinc.value)}
+
     def set_profile(self, enable: bool = True) -> None:
         _check(library().cs_prepared_set_profile(self.handle, int(enable)))
 
     def stage_ms(self) -> dict[str, float]:
         """Device time of each stage of the last profiled run (CUDA events)."""
-        out = (ctypes.c_float * 8)()
-        count = library().cs_prepared_stage_ms(self.handle, out, 8)
+        out = (ctypes.c_float * 16)()
+        count = library().cs_prepared_stage_ms(self.handle, out, 16)
         if count < 0:
             _check(1)
         return {library().cs_stage_name(i).decode(): float(out[i]) for i in range(count)}
@@ -208,6 +228,11 @@ class Renderer:
 
     def set_scratch_limit(self, nbytes: int) -> None:
         _check(library().cs_renderer_set_scratch_limit(self.handle, nbytes))
+
+    def set_shared_sources(self, enable: bool) -> None:
+        """Render each voice source shared by several voices once per batch (the
+        default), or resample every voice frame inline (the plain path)."""
+        _check(library().cs_renderer_set_shared_sources(self.handle, int(enable)))
 
     def prepare(self, plans: list[Plan]) -> Prepared:
         return Prepared(self, plans)

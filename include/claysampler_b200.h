@@ -258,6 +258,26 @@ size_t cs_prepared_segments(const cs_prepared* batch);
  * (docs/validation.md:145). */
 int cs_renderer_set_scratch_limit(cs_renderer* renderer, size_t bytes);
 
+/* Shared voice sources (on by default).  No counterpart in the reference, whose
+ * renderTiles / renderFilterSources resample every voice frame (src/cuda/render.cu:
+ * 138-215).  Voices without a filter chain that play the same sample from the same
+ * position at the same step, with the same loop, loop crossfade and pitch ramp,
+ * have the same resampled source at every elapsed frame; with this on, a batch
+ * renders each such source once (48-tap sinc, loop wrap and crossfade) and the
+ * mix reads it for every voice that plays it.  The audio is identical either way
+ * (the same arithmetic on the same values); off is the plain path, which
+ * resamples every voice frame inline.  Applies to batches prepared afterwards. */
+int cs_renderer_set_shared_sources(cs_renderer* renderer, int enable);
+/* Shared sources of a prepared batch, the floats they hold, and the voice frames
+ * that read them instead of resampling. */
+size_t cs_prepared_shared_sources(const cs_prepared* prepared);
+size_t cs_prepared_shared_frames(const cs_prepared* prepared);
+long long cs_prepared_shared_voice_frames(const cs_prepared* prepared);
+/* Channel-frames of the shared sources that run the 48-tap sinc (step or pitch
+ * ramp away from 1); `voice_floats` receives those of the voices reading them,
+ * which the mix no longer resamples. */
+long long cs_prepared_shared_sinc(const cs_prepared* prepared, long long* voice_floats);
+
 /* ---- natural-tail finishing without device allocation --------------------------
  * No counterpart in the reference (its finishing always runs inside the renderer
  * on renderer-owned scratch).  For callers that cannot allocate device memory

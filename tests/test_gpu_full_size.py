@@ -1,0 +1,106 @@
+"""GPU parity on the benchmarked workloads, at full size.
+
+The cases of tests/test_gpu_parity.py are small; these render the first 64 jobs of
+the 1024-job uneven batch (the default bench workload) and eight full-length jobs
+of the 64-job filtered batch's real preset (88 keys x 4 layers, stereo 24-bit,
+loops, lpf_2p + filter envelope + LFO, pedal), planned by the reference's own
+planner (oracle/_ref), and compare the GPU render with the reference's render.cu
+built for the host plus the oracle's tail.cu restatement.  The shared voice
+sources (one resampling per distinct source, read by every voice that plays it)
+must leave the render bit-identical to the plain path that resamples every voice
+frame.
+
+Tolerances as in tests/test_gpu_parity.py: float bus <= 1e-5 FS, PCM16 <= 1 LSB
+with >= 99.9 % identical, statuses, frames, fades and offsets exact.
+"""
+import numpy as np
+import pytest
+
+from conftest import gpu_available
+from test_gpu_parity import BUS_TOLERANCE, compare_pcm, compare_results
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not gpu_available(), reason="needs a CUDA GPU")]
+
+
+def render(plans, bank, shared=True):
+    from claysampler_b200.renderer import Renderer
+    renderer = Renderer(natural=True)
+    renderer.upload_samples(bank)
+    renderer.set_shared_sources(shared)
+    prepared = renderer.prepare(plans)
+    prepared.run()
+    pcm, results = prepared.collect()
+    mix = prepared.mix()
+    info = prepared.shared
+    prepared.close()
+    renderer.close()
+    return mix, pcm, results, info
+
+
+@pytest.fixture(scope="module")
+def uneven_jobs(tmp_path_factory):
+    from claysampler_b200 import workload
+    return workload.write_uneven_batch(tmp_path_factory.mktemp("uneven"), seed=2, jobs=1024)[:64]
+
+
+@pytest.fixture(scope="module")
+def plain_batch_jobs(tmp_path_factory):
+    from claysampler_b200 import workload
+    return workload.write_plain_batch(tmp_path_factory.mktemp("plain_batch"), seed=2, jobs=8)
+
+
+def check_against_reference(plans, bank, mix, pcm, results):
+    from oracle import oracle, reference
+    expected_mix = reference.synthesize(plans, bank, True)
+    err = float(np.max(np.abs(mix - expected_mix)))
+    assert err <= BUS_TOLERANCE, err
+    expected_pcm, expected = oracle.finish(expected_mix, plans)
+    compare_results(results, expected)
+    compare_pcm(pcm, expected_pcm)
+
+
+def test_uneven_batch_first_64_jobs(uneven_jobs, ref_session):
+    plans = [ref_session.plan(j.sfz, j.midi) for j in uneven_jobs]
+    bank = ref_session.bank()
+    mix, pcm, results, info = render(plans, bank, shared=True)
+    assert info["sources"] > 0 and info["voice_frames"] > 0, info
+    check_against_reference(plans, bank, mix, pcm, results)
+    plain_mix, plain_pcm, plain_results, plain_info = render(plans, bank, shared=False)
+    assert plain_info["sources"] == 0
+    # Shared sources change nothing: same arithmetic on the same values.
+    assert np.array_equal(plain_mix.view(np.uint32), mix.view(np.uint32))
+    assert np.array_equal(plain_pcm, pcm)
+    for field in ("status", "frames", "dataFrames", "fade", "offset", "peak", "first", "last"):
+        np.testing.assert_array_equal(plain_results[field], results[field], err_msg=field)
+
+
+def test_plain_batch_eight_full_jobs(plain_batch_jobs, ref_session):
+    plans = [ref_session.plan(j.sfz, j.midi) for j in plain_batch_jobs]
+    assert all(p.filter_tracks > 0 for p in plans)
+    assert sum(p.frames for p in plans) > 8 * 10 * 44100
+    bank = ref_session.bank()
+    mix, pcm, results, _ = render(plans, bank)
+    check_against_reference(plans, bank, mix, pcm, results)
+
+
+def test_generators_match_reference(tmp_path, ref_session):
+    """sample=*sine and *noise regions (the generator branch of render.cu:80-83),
+    inline and through a filter, at a transposed pitch."""
+    from claysampler_b200 import workload
+    sfz = tmp_path / "generators.sfz"
+    sfz.write_text("<group> ampeg_attack=0.002 ampeg_release=0.2\n"
+                   "<region> sample=*sine lokey=40 hikey=59 pitch_keycenter=52\n"
+                   "<region> sample=*noise lokey=60 hikey=69 volume=-12\n"
+                   "<region> sample=*sine lokey=70 hikey=90 fil_type=lpf_2p cutoff=900 pitch_keycenter=75\n",
+                   encoding="ascii")
+    notes = [(0.05, 0.4, 45, 100), (0.2, 0.3, 62, 90), (0.35, 0.5, 77, 80), (0.5, 0.2, 52, 110),
+             (0.6, 0.6, 66, 70), (0.7, 0.3, 88, 120)]
+    midi = tmp_path / "generators.mid"
+    workload._note_midi(notes, [], 1.5, midi)
+    plans = [ref_session.plan(sfz, midi)]
+    spans = plans[0].spans
+    assert set(spans["generator"].tolist()) >= {1, 3}
+    bank = ref_session.bank()
+    for shared in (True, False):
+        mix, pcm, results, _ = render(plans, bank, shared=shared)
+        check_against_reference(plans, bank, mix, pcm, results)
