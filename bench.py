@@ -23,7 +23,9 @@ batch (no collective), so scaling is weak.
 `cpu_baseline` and `parity` (one rank): the first jobs of the workload planned by
 the reference's own planner and rendered by the reference's render.cu built for
 the host (oracle/_ref, all cores) with the oracle's tail.cu restatement; the GPU
-renders the same reference plans, and `parity` compares the two.
+renders the same reference plans, and `parity` compares that render with the
+reference's own render.cu kernels run on the same GPU (oracle/ref/ref_gpu.cu) and
+with the host build.
 
 `--learned` trains and scores the note-lifetime predictor.  `--serve` measures
 the submit-to-publish latency of requests that arrive one at a time (Poisson)
@@ -316,8 +318,9 @@ def cpu_baseline(jobs, sample_jobs, host_plans, host_bank, renderer):
     host, all cores) over the first `sample_jobs` jobs, and the parity of this
     package on the same jobs: its planner's plans byte for byte against the
     reference planner's, and the GPU render of the reference's plans against the
-    reference's render (float bus error in full scale, PCM16 LSBs, statuses and
-    frames)."""
+    reference's own render.cu kernels on this GPU (the oracle the contract names)
+    and against its host build (float bus error in full scale, PCM16 LSBs,
+    statuses and frames)."""
     threads = os.cpu_count() or 1
     sample = jobs[:sample_jobs]
     plans, bank, render = reference_render(sample, threads)
@@ -333,23 +336,41 @@ def cpu_baseline(jobs, sample_jobs, host_plans, host_bank, renderer):
         gpu_mix = prepared.mix()
     finally:
         prepared.close()
-    diff = np.abs(gpu_pcm.astype(np.int32) - pcm.astype(np.int32)) if gpu_pcm.shape == pcm.shape else None
     same_plans = all(a.to_blob() == b.to_blob() for a, b in zip(host_plans[:len(plans)], plans))
     # The renderer holds this package's bank; the reference plans index the
     # reference's, which must be the same floats.
     same_plans = same_plans and bank.size <= host_bank.size and np.array_equal(bank, host_bank[:bank.size])
+
+    def agreement(ref_mix, ref_pcm, ref_results):
+        diff = np.abs(gpu_pcm.astype(np.int32) - ref_pcm.astype(np.int32)) if gpu_pcm.shape == ref_pcm.shape else None
+        out = {"max_bus_error_fs": float(np.max(np.abs(gpu_mix - ref_mix))) if gpu_mix.shape == ref_mix.shape else None,
+               "bus_bit_identical": bool(gpu_mix.shape == ref_mix.shape
+                                         and np.array_equal(gpu_mix.view(np.uint32), ref_mix.view(np.uint32))),
+               "max_lsb": int(diff.max(initial=0)) if diff is not None else None,
+               "identical_fraction": float(np.mean(diff == 0)) if diff is not None and diff.size else None,
+               "statuses_equal": bool(np.array_equal(gpu_results["status"], ref_results["status"])),
+               "frames_equal": bool(np.array_equal(gpu_results["frames"], ref_results["frames"]))}
+        out["ok"] = bool(out["statuses_equal"] and out["frames_equal"] and out["max_bus_error_fs"] is not None
+                         and out["max_bus_error_fs"] <= 1e-5 and out["max_lsb"] is not None and out["max_lsb"] <= 1
+                         and (out["identical_fraction"] or 1.0) >= 0.999)
+        return out
+
+    host = agreement(mix, pcm, results)
+    host["against"] = "the reference's render.cu built for the host (host libm, no FMA contraction)"
     parity = {"jobs": len(plans), "plans_identical": bool(same_plans),  # plans and sample bank
-              "max_bus_error_fs": float(np.max(np.abs(gpu_mix - mix))) if gpu_mix.shape == mix.shape else None,
-              "max_lsb": int(diff.max()) if diff is not None and diff.size else (0 if diff is not None else None),
-              "identical_fraction": float(np.mean(diff == 0)) if diff is not None and diff.size else None,
-              "statuses_equal": bool(np.array_equal(gpu_results["status"], results["status"])),
-              "frames_equal": bool(np.array_equal(gpu_results["frames"], results["frames"])),
-              "against": "the reference's planner + render.cu on the host + the oracle's tail.cu restatement",
-              "bounds": "bus <= 1e-5 FS, PCM16 <= 1 LSB with >= 99.9 % identical, statuses and frames exact"}
-    parity["ok"] = bool(parity["plans_identical"] and parity["statuses_equal"] and parity["frames_equal"]
-                        and parity["max_bus_error_fs"] is not None and parity["max_bus_error_fs"] <= 1e-5
-                        and parity["max_lsb"] is not None and parity["max_lsb"] <= 1
-                        and (parity["identical_fraction"] or 1.0) >= 0.999)
+              "bounds": "bus <= 1e-5 FS, PCM16 <= 1 LSB with >= 99.9 % identical, statuses and frames exact",
+              "host_reference": host}
+    from oracle import oracle, reference
+    if reference.gpu_available():
+        ref_mix = reference.synthesize_gpu(plans, bank)
+        ref_pcm, ref_results = oracle.finish(ref_mix, plans)
+        device = agreement(ref_mix, ref_pcm, ref_results)
+        device["against"] = "the reference's own render.cu kernels on this GPU (NVRTC defaults: FMA contraction)"
+        parity["gpu_reference"] = device
+        parity["ok"] = bool(same_plans and device["ok"])
+    else:
+        parity["ok"] = bool(same_plans and host["ok"])
+    parity["finishing"] = "the oracle's restatement of tail.cu on the reference's mix"
     return baseline, parity
 
 

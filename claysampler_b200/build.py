@@ -48,7 +48,7 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
             + [ROOT / "include" / "claysampler_b200.h", ROOT / "include" / "claysampler_lifetime.h"])
     if force or _stale(LIBRARY, deps):
         tmp = LIBRARY.with_suffix(f".so.tmp{os.getpid()}")
-        cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
+        cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
                "-Xptxas", "-v" if verbose else "-O3", "-shared", "-o", str(tmp), *map(str, sources)]
         _run(cmd)
         os.replace(tmp, LIBRARY)

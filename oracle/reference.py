@@ -18,15 +18,17 @@ from claysampler_b200.plans import Plan, c_plans
 
 HERE = Path(__file__).resolve().parent
 REF_DIR = HERE / "_ref"
-REFERENCE_ROOT = Path(os.environ.get("CLAY_REFERENCE_ROOT", "/root/reference"))
 TAIL = {"natural": 0, "orig": 1, "custom": 2}
 
 
-def build(quiet: bool = True) -> bool:
-    """Compile oracle/_ref from the reference sources if they are present here."""
-    if not (REFERENCE_ROOT / "src" / "cuda" / "render.cu").exists():
+def build(root=None, quiet: bool = True) -> bool:
+    """Compile oracle/_ref from the reference checkout at `root` (default: the
+    CLAY_REFERENCE_ROOT environment variable) when its sources are present; without
+    them the prebuilt oracle/_ref is used as it is."""
+    root = root or os.environ.get("CLAY_REFERENCE_ROOT")
+    if not root or not (Path(root) / "src" / "cuda" / "render.cu").exists():
         return available()
-    result = subprocess.run(["make", "-s", "-C", str(HERE / "ref"), f"REF={REFERENCE_ROOT}"],
+    result = subprocess.run(["make", "-s", "-C", str(HERE / "ref"), f"REF={root}"],
                             capture_output=quiet, text=True)
     if result.returncode:
         raise RuntimeError("oracle/_ref build failed:\n" + (result.stdout or "") + (result.stderr or ""))
@@ -38,6 +40,36 @@ def available() -> bool:
 
 
 _lib = None
+_gpu = None
+
+
+def gpu_available() -> bool:
+    return (REF_DIR / "libclayref_gpu.so").exists()
+
+
+def gpu_lib():
+    global _gpu
+    if _gpu is None:
+        if not gpu_available():
+            raise RuntimeError("oracle/_ref/libclayref_gpu.so is not built")
+        _gpu = ctypes.CDLL(str(REF_DIR / "libclayref_gpu.so"))
+        _gpu.ref_gpu_last_error.restype = ctypes.c_char_p
+        _gpu.ref_gpu_synthesize.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t,
+                                            ctypes.c_void_p]
+    return _gpu
+
+
+def synthesize_gpu(plans: list[Plan], bank: np.ndarray) -> np.ndarray:
+    """The reference's own render kernels (src/cuda/render.cu built for the GPU with
+    its NVRTC defaults) on the current CUDA device: the float mix, (frames, 2)."""
+    frames = sum(p.frames for p in plans)
+    out = np.zeros((frames, 2), np.float32)
+    array = c_plans(plans)
+    bank = np.ascontiguousarray(bank, np.float32)
+    if gpu_lib().ref_gpu_synthesize(array, len(plans), bank.ctypes.data if bank.size else None, bank.size,
+                                    out.ctypes.data):
+        raise RuntimeError(gpu_lib().ref_gpu_last_error().decode())
+    return out
 
 
 def lib():

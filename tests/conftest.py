@@ -48,3 +48,14 @@ def ref_session():
     session = reference.RefSession()
     yield session
     session.close()
+
+
+def reference_mix(plans, bank, natural=True):
+    """The reference's float mix of `plans`: its own render.cu kernels on the GPU
+    (the contract's oracle, built with its NVRTC defaults) where that build exists,
+    else its render.cu built for the host.  Orig/custom (PCM16) mixes come from the
+    host build."""
+    from oracle import reference
+    if natural and reference.gpu_available() and gpu_available():
+        return reference.synthesize_gpu(plans, bank)
+    return reference.synthesize(plans, bank, natural)

@@ -4,14 +4,19 @@ The cases of tests/test_gpu_parity.py are small; these render the first 64 jobs 
 the 1024-job uneven batch (the default bench workload) and eight full-length jobs
 of the 64-job filtered batch's real preset (88 keys x 4 layers, stereo 24-bit,
 loops, lpf_2p + filter envelope + LFO, pedal), planned by the reference's own
-planner (oracle/_ref), and compare the GPU render with the reference's render.cu
-built for the host plus the oracle's tail.cu restatement.  The shared voice
+planner (oracle/_ref), and compare the GPU render with the reference's own render
+kernels run on the same GPU (src/cuda/render.cu built with its NVRTC defaults,
+oracle/ref/ref_gpu.cu) plus the oracle's tail.cu restatement.  The shared voice
 sources (one resampling per distinct source, read by every voice that plays it)
 must leave the render bit-identical to the plain path that resamples every voice
 frame.
 
 Tolerances as in tests/test_gpu_parity.py: float bus <= 1e-5 FS, PCM16 <= 1 LSB
-with >= 99.9 % identical, statuses, frames, fades and offsets exact.
+with >= 99.9 % identical, statuses, frames, fades and offsets exact.  Against the
+reference's GPU render the float bus is in fact bit-identical, and that is pinned
+too.  (The reference's render.cu built for the host, with the host's libm and no
+FMA contraction, differs from the reference's own GPU render by up to 1.3e-5 FS on
+the full-length filtered jobs, so the GPU render is the oracle here.)
 """
 import numpy as np
 import pytest
@@ -49,14 +54,21 @@ def plain_batch_jobs(tmp_path_factory):
     return workload.write_plain_batch(tmp_path_factory.mktemp("plain_batch"), seed=2, jobs=8)
 
 
-def check_against_reference(plans, bank, mix, pcm, results):
+def check_against_reference(plans, bank, mix, pcm, results, exact=True):
+    """The render against the reference's own kernels on this GPU: within the
+    contract, and (`exact`) bit-identical."""
     from oracle import oracle, reference
-    expected_mix = reference.synthesize(plans, bank, True)
+    if not reference.gpu_available():
+        pytest.skip("oracle/_ref/libclayref_gpu.so (the reference's kernels built for the GPU) is not built")
+    expected_mix = reference.synthesize_gpu(plans, bank)
     err = float(np.max(np.abs(mix - expected_mix)))
     assert err <= BUS_TOLERANCE, err
     expected_pcm, expected = oracle.finish(expected_mix, plans)
     compare_results(results, expected)
     compare_pcm(pcm, expected_pcm)
+    if exact:
+        assert np.array_equal(mix.view(np.uint32), expected_mix.view(np.uint32)), f"bus differs by up to {err}"
+        assert np.array_equal(pcm, expected_pcm)
 
 
 def test_uneven_batch_first_64_jobs(uneven_jobs, ref_session):

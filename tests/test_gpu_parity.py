@@ -1,6 +1,7 @@
-"""GPU parity: the sm_100a render path against the reference's own host render
-(oracle/_ref: the reference planner and src/cuda/render.cu compiled for the CPU)
-and the plain-C restatement of its finishing stages (oracle/).
+"""GPU parity: the sm_100a render path against the reference's own render
+(oracle/_ref: the reference planner, and src/cuda/render.cu run as the reference
+runs it on this GPU, or compiled for the CPU where no GPU build exists) and the
+plain-C restatement of its finishing stages (oracle/).
 
 Tolerances (the contract for this path): float bus max |error| <= 1e-5 of full
 scale; PCM16 within 1 LSB with >= 99.9 % of samples identical; tail frame indices,
@@ -9,7 +10,7 @@ output lengths and statuses bit-exact.
 import numpy as np
 import pytest
 
-from conftest import gpu_available
+from conftest import gpu_available, reference_mix
 
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not gpu_available(), reason="needs a CUDA GPU")]
@@ -59,7 +60,7 @@ def test_plain_small_matches_reference(plain_small, ref_session, tail):
     bank = ref_session.bank()
     natural = tail == "natural"
     mix, pcm, results, _ = render(plans, bank, natural)
-    ref_mix = reference.synthesize(plans, bank, natural)
+    ref_mix = reference_mix(plans, bank, natural)
     if natural:
         err = float(np.max(np.abs(mix - ref_mix)))
         assert err <= BUS_TOLERANCE, err
@@ -78,7 +79,7 @@ def test_filtered_batch_matches_reference(batch_mini, ref_session, tail):
     bank = ref_session.bank()
     natural = tail == "natural"
     mix, pcm, results, _ = render(plans, bank, natural)
-    ref_mix = reference.synthesize(plans, bank, natural)
+    ref_mix = reference_mix(plans, bank, natural)
     if natural:
         err = float(np.max(np.abs(mix - ref_mix)))
         assert err <= BUS_TOLERANCE, err
@@ -201,7 +202,7 @@ def test_transposed_stereo_matches_reference(ref_session, tmp_path):
     assert odd.any(), "no stereo sample at an odd float offset"
     bank = ref_session.bank()
     mix, pcm, results, _ = render(plans, bank, True)
-    ref_mix = reference.synthesize(plans, bank, True)
+    ref_mix = reference_mix(plans, bank, True)
     err = float(np.max(np.abs(mix - ref_mix)))
     assert err <= BUS_TOLERANCE, err
     ref_pcm, ref_results = oracle.finish(ref_mix, plans, True)
