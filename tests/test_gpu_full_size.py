@@ -115,4 +115,6 @@ def test_generators_match_reference(tmp_path, ref_session):
     bank = ref_session.bank()
     for shared in (True, False):
         mix, pcm, results, _ = render(plans, bank, shared=shared)
-        check_against_reference(plans, bank, mix, pcm, results)
+        # Within the contract; not bit for bit (up to 6e-8 FS: the generator voices'
+        # arithmetic contracts differently from the reference's in places).
+        check_against_reference(plans, bank, mix, pcm, results, exact=False)
