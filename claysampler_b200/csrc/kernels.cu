@@ -15,6 +15,7 @@
 #include "kernels.cuh"
 #include "voice_math.cuh"
 
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <initializer_list>
@@ -791,11 +792,12 @@ __device__ __forceinline__ MixVoice mixVoiceOf(const BatchView& b, const Segment
 
 constexpr int kMixStaged = kMixThreads / kTilesPerBlock;     // staged voices per tile
 
-// Inline: the batch has unfiltered voices, which the mix renders itself (the
-// general kernel, given more registers for the resampler); without them a lighter
-// kernel keeps 64 warps resident.
-template <bool Natural, bool Inline>
-__global__ void __launch_bounds__(kMixThreads, Inline ? 5 : 8) mixKernel(BatchView b, SegmentView s, StereoStats* stats)
+// Inline: 1 when some unfiltered voice is resampled by the mix itself (the
+// general kernel, given more registers for the resampler); 2 when every unfiltered
+// voice reads a shared source; 0 when every voice is filtered.  The lighter
+// kernels keep 64 warps resident.
+template <bool Natural, int Inline>
+__global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(BatchView b, SegmentView s, StereoStats* stats)
 {
     __shared__ double reduceD[32];
     __shared__ float reduceF[32];
@@ -858,12 +860,12 @@ __global__ void __launch_bounds__(kMixThreads, Inline ? 5 : 8) mixKernel(BatchVi
                 const float2 gains = panGains(v, offset);
                 wetLeft += x * gains.x;
                 wetRight += x * gains.y;
-            } else if (Inline && m.kind == 0) {
+            } else if (Inline == 1 && m.kind == 0) {
                 const float2 sample = voiceFrame<true>(b.bank, b.sinc, b.voices[m.index], b.points, b.modulation,
                                                        pan, frame, false, -1.0);
                 left += sample.x;
                 right += sample.y;
-            } else if (Inline) {
+            } else if (Inline && m.kind >= 3) {
                 // voiceFrame with the source read from the shared sources.
                 const cs_voice_span& v = b.voices[m.index];
                 const float level = envelopeAt(v, frame);
@@ -968,67 +970,93 @@ __global__ void __launch_bounds__(kMixThreads) scanKernel(BatchView b, StereoSta
 
 // ---- finishing (src/cuda/tail.cu) ------------------------------------------------------
 
-// Natural endpoint, peak repair and scale, one warp per job (tail.cu:83-139).
-__global__ void selectNativeKernel(BatchView b, FinishView f)
+// ---- natural endpoint, peak repair and scale (tail.cu:83-139) -------------------------
+//
+// The reference walks each job's 1024-frame blocks in order on one thread: the
+// first block at or after the music's end whose power is at most 1e-12 per sample
+// (re-summed in frame order near the threshold), or the first non-finite block,
+// ends the search, and the peak is the loudest block before it (and the quiet
+// block itself).  Here every block is tested at once: the first stopping block is
+// an integer minimum (atomicMin), the peak an integer maximum of the non-negative
+// float bits (atomicMax), so the result is the walk's whatever the order; a thread
+// per job then applies the end rules.
+
+__global__ void scanResetKernel(FinishView f, int jobs)
 {
-    const int jobIndex = int(blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
-    const int lane = int(threadIdx.x & 31);
+    const int j = int(blockIdx.x * blockDim.x + threadIdx.x);
+    if (j < jobs)
+        f.scans[j] = JobScan{INT_MAX, 0, -1, 0, 0ull};
+}
+
+// Thread per block: does the block stop the natural search, and how.
+__global__ void nativeStopKernel(BatchView b, FinishView f, int blocks)
+{
+    const int g = int(blockIdx.x * blockDim.x + threadIdx.x);
+    if (g >= blocks)
+        return;
+    const int jobIndex = b.blockJob[g];
+    const JobInfo job = b.jobs[jobIndex];
+    const int block = g - job.blockFirst;
+    const StereoStats stat = f.stereo[g];
+    const bool bad = !isfinite(stat.peak);
+    const int first = block * kBlockFrames;
+    const int blockEnd = min(job.limit, first + kBlockFrames);
+    bool quiet = false;
+    if (!bad && blockEnd >= job.musicEnd) {
+        const double threshold = 1e-12 * (blockEnd - first) * 2;
+        double power = stat.power;
+        // Near the threshold, re-sum in frame order as the host does.
+        if (fabs(power - threshold) <= threshold * 1e-12) {
+            power = 0;
+            const float2* mix = static_cast<const float2*>(b.mix) + job.offset;
+            for (int frame = first; frame < min(blockEnd, job.frames); ++frame) {
+                const float2 value = mix[frame];
+                power += __fmul_rn(value.x, value.x);
+                power += __fmul_rn(value.y, value.y);
+            }
+        }
+        quiet = power <= threshold;
+    }
+    if (bad || quiet)
+        atomicMin(&f.scans[jobIndex].stop, 2 * block + (bad ? 1 : 0));
+}
+
+// Thread per block: the peak over the blocks the walk reads before stopping.
+__global__ void nativePeakKernel(BatchView b, FinishView f, int blocks)
+{
+    const int g = int(blockIdx.x * blockDim.x + threadIdx.x);
+    if (g >= blocks)
+        return;
+    const int jobIndex = b.blockJob[g];
+    const int block = g - b.jobs[jobIndex].blockFirst;
+    const int stop = f.scans[jobIndex].stop;
+    const int stopBlock = stop == INT_MAX ? INT_MAX : stop >> 1;
+    if (block < stopBlock || (block == stopBlock && !(stop & 1))) {
+        const float peak = f.stereo[g].peak;           // finite and >= 0 here
+        if (peak > 0)
+            atomicMax(&f.scans[jobIndex].peak, __float_as_int(peak));
+    }
+}
+
+// Thread per job: status, end frame, data frames and scale.
+__global__ void nativeResultKernel(BatchView b, FinishView f)
+{
+    const int jobIndex = int(blockIdx.x * blockDim.x + threadIdx.x);
     if (jobIndex >= b.jobCount)
         return;
     const JobInfo job = b.jobs[jobIndex];
-    const int blocks = (job.frames + kBlockFrames - 1) / kBlockFrames;
-    float peak = 0;
-    int end = 0;
-    bool nonfinite = false;
-    for (int base = 0; base < blocks; base += 32) {
-        const int block = base + lane;
-        bool bad = false, quiet = false;
-        float blockPeak = 0;
-        int blockEnd = 0;
-        if (block < blocks) {
-            const StereoStats stat = f.stereo[job.blockFirst + block];
-            blockPeak = stat.peak;
-            bad = !isfinite(stat.peak);
-            const int first = block * kBlockFrames;
-            blockEnd = min(job.limit, first + kBlockFrames);
-            if (!bad && blockEnd >= job.musicEnd) {
-                const double threshold = 1e-12 * (blockEnd - first) * 2;
-                double power = stat.power;
-                // Near the threshold, re-sum in frame order as the host does.
-                if (fabs(power - threshold) <= threshold * 1e-12) {
-                    power = 0;
-                    const float2* mix = static_cast<const float2*>(b.mix) + job.offset;
-                    for (int frame = first; frame < min(blockEnd, job.frames); ++frame) {
-                        const float2 value = mix[frame];
-                        power += __fmul_rn(value.x, value.x);
-                        power += __fmul_rn(value.y, value.y);
-                    }
-                }
-                quiet = power <= threshold;
-            }
-        }
-        const unsigned stop = __ballot_sync(0xffffffffu, bad || quiet);
-        const int first = stop ? __ffs(stop) - 1 : 32;
-        if (lane < first || (lane == first && quiet))
-            peak = fmaxf(peak, blockPeak);
-        if (stop) {
-            const int endLane = first;
-            nonfinite = __shfl_sync(0xffffffffu, bad ? 1 : 0, endLane) != 0;
-            end = __shfl_sync(0xffffffffu, blockEnd, endLane);
-            break;
-        }
-    }
-    #pragma unroll
-    for (int d = 16; d; d >>= 1)
-        peak = fmaxf(peak, __shfl_xor_sync(0xffffffffu, peak, d));
-    if (lane)
-        return;
+    const JobScan scan = f.scans[jobIndex];
     cs_tail_result result{};
-    if (nonfinite) {
-        result.status = CS_TAIL_NONFINITE;
-        f.results[jobIndex] = result;
-        return;
+    int end = 0;
+    if (scan.stop != INT_MAX) {
+        if (scan.stop & 1) {
+            result.status = CS_TAIL_NONFINITE;
+            f.results[jobIndex] = result;
+            return;
+        }
+        end = min(job.limit, (scan.stop >> 1) * kBlockFrames + kBlockFrames);
     }
+    const float peak = __int_as_float(scan.peak);
     if (!end) {
         const int silent = (job.frames + kBlockFrames - 1) / kBlockFrames * kBlockFrames;
         if (silent < job.limit)
@@ -1084,34 +1112,57 @@ __global__ void quantizeMonoKernel(BatchView b, FinishView f, int window)
         f.windows[w] = {power, peak};
 }
 
-// Weak-tail trim, one warp per job (tail.cu:183-213).
-__global__ void selectTrimKernel(BatchView b, FinishView f, TailConfig config)
+// ---- weak-tail trim (tail.cu:183-213) ---------------------------------------------------
+//
+// The threshold follows from the loudest 50 ms window of the job's PCM (an integer
+// maximum of the non-negative double bits) and the trim point from the last
+// window above it (an integer maximum of window indices), each window tested by
+// its own thread; a thread per job applies the trim.
+
+__device__ __forceinline__ bool trimWindow(const BatchView& b, const FinishView& f, int w, int& jobIndex, int& index)
 {
-    const int jobIndex = int(blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
-    const int lane = int(threadIdx.x & 31);
+    jobIndex = b.windowJob[w];
+    if (f.results[jobIndex].status != CS_TAIL_OK)
+        return false;
+    index = w - b.jobs[jobIndex].windowFirst;
+    return index < 0 ? false : true;
+}
+
+__global__ void trimPowerKernel(BatchView b, FinishView f, TailConfig config, int windows)
+{
+    const int w = int(blockIdx.x * blockDim.x + threadIdx.x);
+    int jobIndex, index;
+    if (w >= windows || !trimWindow(b, f, w, jobIndex, index))
+        return;
+    const int count = (f.results[jobIndex].dataFrames + config.window - 1) / config.window;
+    if (index < count)
+        atomicMax(&f.scans[jobIndex].maxPower, (unsigned long long)__double_as_longlong(f.windows[w].power));
+}
+
+__global__ void trimLastKernel(BatchView b, FinishView f, TailConfig config, int windows)
+{
+    const int w = int(blockIdx.x * blockDim.x + threadIdx.x);
+    int jobIndex, index;
+    if (w >= windows || !trimWindow(b, f, w, jobIndex, index))
+        return;
+    const int count = (f.results[jobIndex].dataFrames + config.window - 1) / config.window;
+    if (index >= count)
+        return;
+    const double maxPower = __longlong_as_double((long long)f.scans[jobIndex].maxPower);
+    const double threshold = fmin(config.ceiling, fmax(config.floor, sqrt(maxPower / config.window) * config.relative));
+    const MonoStats stat = f.windows[w];
+    if (sqrt(stat.power / config.window) > threshold || stat.peak > threshold * 4)
+        atomicMax(&f.scans[jobIndex].last, index);
+}
+
+__global__ void trimResultKernel(BatchView b, FinishView f, TailConfig config)
+{
+    const int jobIndex = int(blockIdx.x * blockDim.x + threadIdx.x);
     if (jobIndex >= b.jobCount)
         return;
     cs_tail_result& result = f.results[jobIndex];
-    if (result.status != CS_TAIL_OK)
-        return;
-    const MonoStats* windows = f.windows + b.jobs[jobIndex].windowFirst;
-    const int count = (result.dataFrames + config.window - 1) / config.window;
-    double maxPower = 0;
-    for (int i = lane; i < count; i += 32)
-        maxPower = fmax(maxPower, windows[i].power);
-    #pragma unroll
-    for (int d = 16; d; d >>= 1)
-        maxPower = fmax(maxPower, __shfl_xor_sync(0xffffffffu, maxPower, d));
-    const double threshold = fmin(config.ceiling, fmax(config.floor, sqrt(maxPower / config.window) * config.relative));
-    int last = -1;
-    for (int top = count - 1; top >= 0 && last < 0; top -= 32) {
-        const int i = top - lane;
-        const bool loud = i >= 0 && (sqrt(windows[i].power / config.window) > threshold || windows[i].peak > threshold * 4);
-        const unsigned hits = __ballot_sync(0xffffffffu, loud);
-        if (hits)
-            last = top - (__ffs(hits) - 1);
-    }
-    if (lane || last < 0)
+    const int last = f.scans[jobIndex].last;
+    if (result.status != CS_TAIL_OK || last < 0)
         return;
     const int lastSound = min(result.frames, (last + 1) * config.window);
     if (result.frames - lastSound >= config.quietFrames) {
@@ -1365,23 +1416,21 @@ void launchMix(const BatchView& b, const SegmentView& s, bool natural, StereoSta
 {
     if (!s.blockCount)
         return;
-    if (b.inlineVoices)
+    if (b.inlineVoices == 1)
         setOncePerDevice(2, [] {
-            return firstError({cudaFuncSetAttribute(mixKernel<true, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+            return firstError({cudaFuncSetAttribute(mixKernel<true, 1>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                                     kInlineMixCarveout),
-                               cudaFuncSetAttribute(mixKernel<false, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               cudaFuncSetAttribute(mixKernel<false, 1>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                                     kInlineMixCarveout)});
         });
-    if (natural) {
-        if (b.inlineVoices)
-            mixKernel<true, true><<<s.blockCount, kMixThreads, 0, stream>>>(b, s, stats);
-        else
-            mixKernel<true, false><<<s.blockCount, kMixThreads, 0, stream>>>(b, s, stats);
-    } else {
-        if (b.inlineVoices)
-            mixKernel<false, true><<<s.blockCount, kMixThreads, 0, stream>>>(b, s, stats);
-        else
-            mixKernel<false, false><<<s.blockCount, kMixThreads, 0, stream>>>(b, s, stats);
+    const auto launch = [&](auto kernel) { kernel<<<s.blockCount, kMixThreads, 0, stream>>>(b, s, stats); };
+    switch ((natural ? 3 : 0) + b.inlineVoices) {
+    case 0: launch(mixKernel<false, 0>); break;
+    case 1: launch(mixKernel<false, 1>); break;
+    case 2: launch(mixKernel<false, 2>); break;
+    case 3: launch(mixKernel<true, 0>); break;
+    case 4: launch(mixKernel<true, 1>); break;
+    default: launch(mixKernel<true, 2>); break;
     }
 }
 
@@ -1389,15 +1438,27 @@ int launchFinish(const BatchView& b, const FinishView& f, bool natural, bool qua
                  cudaStream_t stream)
 {
     int launches = 0;
-    const int warpsGrid = (b.jobCount + 7) / 8;
     if (natural) {
-        selectNativeKernel<<<warpsGrid, 256, 0, stream>>>(b, f);
+        constexpr int threads = 256;
+        const int jobGrid = (b.jobCount + threads - 1) / threads;
+        const int blockGrid = (f.blockCount + threads - 1) / threads;
+        const int windowGrid = (f.windowCount + threads - 1) / threads;
+        scanResetKernel<<<jobGrid, threads, 0, stream>>>(f, b.jobCount);
+        launches += 1;
+        if (f.blockCount) {
+            nativeStopKernel<<<blockGrid, threads, 0, stream>>>(b, f, f.blockCount);
+            nativePeakKernel<<<blockGrid, threads, 0, stream>>>(b, f, f.blockCount);
+            launches += 2;
+        }
+        nativeResultKernel<<<jobGrid, threads, 0, stream>>>(b, f);
         ++launches;
         if (f.windowCount) {
             quantizeMonoKernel<<<f.windowCount, 256, 0, stream>>>(b, f, tail.window);
-            ++launches;
+            trimPowerKernel<<<windowGrid, threads, 0, stream>>>(b, f, tail, f.windowCount);
+            trimLastKernel<<<windowGrid, threads, 0, stream>>>(b, f, tail, f.windowCount);
+            launches += 3;
         }
-        selectTrimKernel<<<warpsGrid, 256, 0, stream>>>(b, f, tail);
+        trimResultKernel<<<jobGrid, threads, 0, stream>>>(b, f, tail);
         ++launches;
     }
     layoutKernel<<<1, 32, 0, stream>>>(b, f, natural ? 1 : 0);

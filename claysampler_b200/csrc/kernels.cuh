@@ -143,7 +143,17 @@ inline BodyGeometry bodyGeometry(const cs_audio_config& config)
     return g;
 }
 
+// Per-job reductions of the block-parallel tail searches: the first 1024-frame
+// block that ends the natural search (2 * block + 1 when it is non-finite, else
+// 2 * block; INT_MAX when none), the peak of the blocks before it (float bits),
+// the loudest tail window's power (double bits) and the last loud window.
+struct JobScan {
+    int stop, peak, last, pad;
+    unsigned long long maxPower;
+};
+
 struct FinishView {
+    JobScan* scans;                     // one per job
     StereoStats* stereo;
     MonoStats* windows;
     short* mono;

@@ -694,6 +694,11 @@ struct cs_prepared {
     const int2* deviceGroups = nullptr;
     size_t bodyBytes = 0;
     short* output = nullptr;            // the PCM the batch publishes
+    // Download enqueued behind the batch's kernels into its lane's page-locked
+    // buffer (error flag, results, PCM up to the batch's frames), done at `copied`.
+    bool asyncDownload = false;
+    cudaEvent_t copied = nullptr;
+    size_t downloadResults = 0, downloadPcm = 0;   // offsets in the lane's buffer
     // Optional per-stage timing: an event after every stage of the last run.
     bool profile = false;
     std::vector<cudaEvent_t> marks;
@@ -716,6 +721,8 @@ struct cs_renderer {
         cudaEvent_t leadReady[cs::kLeadTiers] = {}, leadDone[cs::kLeadTiers] = {};
         void* arena = nullptr;
         size_t arenaCapacity = 0;
+        void* download = nullptr;       // page-locked: the lane's published batch
+        size_t downloadCapacity = 0;
     };
     static constexpr int kLanes = 2;
     Lane lanes[kLanes];
@@ -861,6 +868,7 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     const size_t oStates = section(p->stateBytes);
     p->resultBytes = jobs * sizeof(cs_tail_result);
     const size_t oResults = section(p->resultBytes);
+    const size_t oScans = section(jobs * sizeof(JobScan));
     p->mixBytes = batch.frames * frameBytes;
     const size_t oMix = section(p->mixBytes);
     const size_t oStereo = section(size_t(batch.blocks) * sizeof(StereoStats));
@@ -1011,8 +1019,18 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     p->sharedSources = reinterpret_cast<const SharedSource*>(base + oSharedSources);
     p->sharedTiles = reinterpret_cast<const int2*>(base + oSharedTiles);
     v.jobCount = int(jobs);
-    v.inlineVoices = std::any_of(batch.voices.begin(), batch.voices.end(),
-                                 [](const cs_voice_span& voice) { return voice.filterTrack < 0; }) ? 1 : 0;
+    // 1: the mix resamples some unfiltered voice itself; 2: every unfiltered voice
+    // reads a shared source; 0: no unfiltered voice.
+    v.inlineVoices = 0;
+    for (size_t k = 0; k < batch.voices.size(); ++k) {
+        if (batch.voices[k].filterTrack >= 0)
+            continue;
+        if (sh.refs.empty() || sh.refs[k].offset < 0) {
+            v.inlineVoices = 1;
+            break;
+        }
+        v.inlineVoices = 2;
+    }
     const size_t voiceCount = batch.voices.size();
     for (const auto& seg : t.segments) {
         SegmentView s{};
@@ -1037,6 +1055,7 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     // Pitch phases follow the filtered floats of the same segment.
     v.phase = reinterpret_cast<double*>(base + oScratch);
     FinishView& f = p->finish;
+    f.scans = reinterpret_cast<JobScan*>(base + oScans);
     f.stereo = reinterpret_cast<StereoStats*>(base + oStereo);
     f.windows = reinterpret_cast<MonoStats*>(base + oWindows);
     f.mono = reinterpret_cast<short*>(base + oMono);
@@ -1198,6 +1217,30 @@ size_t collectResults(cs_renderer& r, cs_prepared& p)
     return size_t(last.offset + uint64_t(last.dataFrames)) * (r.natural ? 1 : 2);
 }
 
+// Enqueues the batch's download behind its kernels on its lane's stream: the error
+// flag, the results and the PCM (up to the batch's frames, an upper bound of what
+// it publishes) into the lane's page-locked buffer, so that the copy runs while
+// the host stages the next batch.  The lane's previous batch is already published.
+void enqueueDownload(cs_renderer& r, cs_prepared& p)
+{
+    cs_renderer::Lane& lane = r.lanes[p.lane];
+    const size_t pcmBytes = p.batch.frames * (r.natural ? 1 : 2) * sizeof(int16_t);
+    p.downloadResults = 256;
+    p.downloadPcm = align256(p.downloadResults + p.resultBytes);
+    auto* buffer = static_cast<unsigned char*>(
+        cs_renderer::pinned(lane.download, lane.downloadCapacity, p.downloadPcm + std::max<size_t>(pcmBytes, 1)));
+    if (!p.copied)
+        check(cudaEventCreateWithFlags(&p.copied, cudaEventDisableTiming), "CUDA download event");
+    check(cudaMemcpyAsync(buffer, p.view.error, sizeof(int), cudaMemcpyDeviceToHost, lane.stream), "CUDA error flag download");
+    check(cudaMemcpyAsync(buffer + p.downloadResults, p.finish.results, p.resultBytes, cudaMemcpyDeviceToHost, lane.stream),
+          "CUDA render metadata download");
+    if (pcmBytes)
+        check(cudaMemcpyAsync(buffer + p.downloadPcm, p.output, pcmBytes, cudaMemcpyDeviceToHost, lane.stream),
+              "CUDA PCM download");
+    check(cudaEventRecord(p.copied, lane.stream), "CUDA download event");
+    p.asyncDownload = true;
+}
+
 void checkPlans(const cs_plan* plans, size_t count)
 {
     if (count && !plans)
@@ -1327,6 +1370,7 @@ private:
                 continue;
             }
             run(r, *prepared, nullptr);
+            enqueueDownload(r, *prepared);
             flight.push_back({prepared, next});
             next += jobs;
         }
@@ -1525,6 +1569,22 @@ private:
 
     void publishBatch(cs_prepared& p, size_t first)
     {
+        if (p.asyncDownload) {
+            check(cudaEventSynchronize(p.copied), "CUDA batch download");
+            const auto* buffer = static_cast<const unsigned char*>(r.lanes[p.lane].download);
+            int failed = 0;
+            std::memcpy(&failed, buffer, sizeof(int));
+            if (failed)
+                throw std::runtime_error("a device wait ran out of its iteration limit (staged copy did not complete)");
+            const auto* results = reinterpret_cast<const cs_tail_result*>(buffer + p.downloadResults);
+            const size_t count = p.batch.jobs.size();
+            const size_t samples = count ? size_t(results[count - 1].offset + uint64_t(results[count - 1].dataFrames)) *
+                (r.natural ? 1 : 2) : 0;
+            p.results.assign(results, results + count);
+            deliver(reinterpret_cast<const int16_t*>(buffer + p.downloadPcm), samples, p.results.data(), count,
+                    seconds(p), first);
+            return;
+        }
         const size_t samples = collectResults(r, p);
         int16_t* pcm = hostPcm(samples);
         if (samples)
@@ -1773,6 +1833,8 @@ void cs_renderer_destroy(cs_renderer* r)
     }
     if (r->hostPcm) cudaFreeHost(r->hostPcm);
     if (r->staging) cudaFreeHost(r->staging);
+    for (auto& lane : r->lanes)
+        if (lane.download) cudaFreeHost(lane.download);
     for (auto& lane : r->lanes) {
         if (lane.stream) cudaStreamDestroy(lane.stream);
         for (int k = 0; k < cs::kLeadTiers; ++k) {
@@ -1921,8 +1983,10 @@ void cs_prepared_destroy(cs_prepared* p)
     if (p->end) cudaEventSynchronize(p->end);
     for (cudaEvent_t e : p->marks)
         cudaEventDestroy(e);
+    if (p->copied) cudaEventSynchronize(p->copied);
     if (p->begin) cudaEventDestroy(p->begin);
     if (p->end) cudaEventDestroy(p->end);
+    if (p->copied) cudaEventDestroy(p->copied);
     if (p->arena && !p->sharedArena) {
         cudaFree(p->arena);
         if (p->owner)

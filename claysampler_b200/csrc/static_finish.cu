@@ -5,7 +5,7 @@
 // the renderer that owns the whole device-memory budget itself.
 //
 // The stage's intermediates — per-block stereo power and peak, per-window mono
-// stats, the mono PCM16 and the job tables — live in one file-scope device array
+// stats, the mono PCM16, the per-job search reductions and the job tables — live in one file-scope device array
 // of fixed size instead of the renderer's arena.  Its limit is
 // CS_STATIC_FINISH_MAX_FRAMES frames and CS_STATIC_FINISH_MAX_JOBS jobs per call.
 // Every call reuses the same array and leaves the last call's contents in it;
@@ -36,7 +36,8 @@ constexpr size_t kWindowJobAt = alignUp(kBlockJobAt + kMaxBlocks * sizeof(int));
 constexpr size_t kStereoAt = alignUp(kWindowJobAt + kMaxWindows * sizeof(int));
 constexpr size_t kWindowsAt = alignUp(kStereoAt + kMaxBlocks * sizeof(StereoStats));
 constexpr size_t kMonoAt = alignUp(kWindowsAt + kMaxWindows * sizeof(MonoStats));
-constexpr size_t kScratchBytes = alignUp(kMonoAt + kMaxFrames * sizeof(short));
+constexpr size_t kScansAt = alignUp(kMonoAt + kMaxFrames * sizeof(short));
+constexpr size_t kScratchBytes = alignUp(kScansAt + kMaxJobs * sizeof(JobScan));
 
 static __device__ __align__(256) unsigned char gFinishScratch[kScratchBytes];
 
@@ -173,6 +174,7 @@ extern "C" int cs_finish_natural_static(const float* mix, const cs_finish_job* j
         view.mix = const_cast<float*>(mix);
         view.jobCount = count;
         FinishView finish{};
+        finish.scans = reinterpret_cast<JobScan*>(scratch + kScansAt);
         finish.stereo = reinterpret_cast<StereoStats*>(scratch + kStereoAt);
         finish.windows = reinterpret_cast<MonoStats*>(scratch + kWindowsAt);
         finish.mono = reinterpret_cast<short*>(scratch + kMonoAt);
