@@ -86,6 +86,9 @@ def parse():
                         "flight overlap one's upload and download with the other's kernels")
     p.add_argument("--no-autotune", action="store_true",
                    help="skip the GPU batch-size sweep and use --e2e-batch-jobs for the end-to-end pass")
+    p.add_argument("--device-only", action="store_true",
+                   help="time only the device step of the batched form (no plain comparison, end-to-end pass or "
+                        "CPU baseline): the command the committed ncu launch lists run")
     p.add_argument("--serve", action="store_true",
                    help="serving run instead: Poisson arrivals through cs_submit / cs_poll, job latency")
     p.add_argument("--learned", action="store_true",
@@ -452,11 +455,13 @@ def run_b200(args):
         return sum(step_ms) / len(step_ms), totals
 
     # The plain path first: every voice frame resampled inline.
-    renderer.set_shared_sources(False)
-    plain = renderer.prepare(plans)
-    plain.set_profile(True)
-    plain_ms, plain_totals = timed(plain)
-    plain.close()
+    plain_ms, plain_totals = float("nan"), {}
+    if not args.device_only:
+        renderer.set_shared_sources(False)
+        plain = renderer.prepare(plans)
+        plain.set_profile(True)
+        plain_ms, plain_totals = timed(plain)
+        plain.close()
     # The batched form: each voice source shared by several voices of the batch
     # rendered once (bit-identical audio).
     renderer.set_shared_sources(True)
@@ -469,6 +474,17 @@ def run_b200(args):
     audio = float(results["frames"].sum()) / RATE
     statuses = np.bincount(results["status"], minlength=12).tolist()
     launches = prepared.launches * args.steps
+    if args.device_only:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "device_only": True, "value": audio / (ms * 1e-3), "unit": "audio-s/s",
+                              "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
+                              "stage_ms": {k: v / args.steps for k, v in stage_totals.items()},
+                              "config": bench_config(args, jobs, world), "gpu_launches": launches}))
+        prepared.close()
+        renderer.close()
+        if distributed:
+            torch.distributed.destroy_process_group()
+        return
 
     # End to end through the public API: plans in host memory, PCM back to host, in
     # GPU batches of the size the autotuner measured fastest for this workload.
