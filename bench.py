@@ -517,6 +517,7 @@ def run_b200(args):
         if i >= args.warmup:
             e2e_times.append(elapsed)
     e2e_s = sum(e2e_times) / len(e2e_times)
+    host_ms = {k: v / (args.warmup + args.steps) for k, v in e2e_renderer.host_ms().items()}
 
     totals = torch.tensor([audio, ms, e2e_s, box.get("audio", 0.0)], dtype=torch.float64, device="cuda")
     total_audio, max_ms, max_e2e, total_e2e_audio = combine(gather_rows(totals, world))
@@ -572,7 +573,7 @@ def run_b200(args):
                "shared_sources": shared_info,
                "e2e": {"value": total_e2e_audio / max_e2e, "unit": "audio-s/s", "h2d_bytes_per_step": int(h2d),
                        "d2h_bytes_per_step": int(box.get("pcm", 0)), "ms_per_step": max_e2e * 1e3,
-                       "batch_jobs": e2e_batch, "autotune": tuned,
+                       "batch_jobs": e2e_batch, "autotune": tuned, "host_staging_ms_per_step": host_ms,
                        "pass_ms": [round(t * 1e3, 2) for t in e2e_times]},
                "gpu_launches": launches, "clocks": clocks.summary()}
         if world == 1:

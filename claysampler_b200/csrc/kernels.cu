@@ -1078,12 +1078,28 @@ __global__ void nativeResultKernel(BatchView b, FinishView f)
     f.results[jobIndex] = result;
 }
 
-// Mono PCM16 with ties-to-even channel average and per-window stats (tail.cu:147-181).
-__global__ void quantizeMonoKernel(BatchView b, FinishView f, int window)
+// Warps per CTA of the warp-per-unit finishing kernels, and a warp-wide reduction.
+constexpr int kFinalizeWarps = 8;
+
+template <class T, class Op>
+__device__ __forceinline__ T warpAll(T value, Op op)
 {
-    __shared__ double reduceD[32];
-    __shared__ int reduceI[32];
-    const int w = int(blockIdx.x);
+    #pragma unroll
+    for (int d = 16; d; d >>= 1)
+        value = op(value, __shfl_xor_sync(0xffffffffu, value, d));
+    return value;
+}
+
+// Mono PCM16 with ties-to-even channel average and per-window stats (tail.cu:147-181).
+// A warp per 50 ms window (eight per CTA).  The window's power is a sum of squared
+// 16-bit integers, below 2^53, so every partial sum is exact and any order gives
+// the reference's double.
+__global__ void __launch_bounds__(kFinalizeWarps * 32) quantizeMonoKernel(BatchView b, FinishView f, int window)
+{
+    const int w = int(blockIdx.x) * kFinalizeWarps + int(threadIdx.x >> 5);
+    const int lane = int(threadIdx.x & 31);
+    if (w >= f.windowCount)
+        return;
     const int jobIndex = b.windowJob[w];
     const JobInfo job = b.jobs[jobIndex];
     const cs_tail_result& result = f.results[jobIndex];
@@ -1096,7 +1112,7 @@ __global__ void quantizeMonoKernel(BatchView b, FinishView f, int window)
     short* mono = f.mono + job.offset;
     double power = 0;
     int peak = 0;
-    for (int frame = first + int(threadIdx.x); frame < end; frame += blockDim.x) {
+    for (int frame = first + lane; frame < end; frame += 32) {
         const float2 sample = mix[frame];
         const int left = __float2int_rn(fminf(32767.f, fmaxf(-32768.f, sample.x * scale)));
         const int right = __float2int_rn(fminf(32767.f, fmaxf(-32768.f, sample.y * scale)));
@@ -1106,9 +1122,9 @@ __global__ void quantizeMonoKernel(BatchView b, FinishView f, int window)
         power += double(value) * value;
         peak = max(peak, abs(value));
     }
-    power = blockReduce(power, 0.0, SumOp{}, reduceD);
-    peak = blockReduce(peak, 0, MaxOp{}, reduceI);
-    if (threadIdx.x == 0)
+    power = warpAll(power, SumOp{});
+    peak = warpAll(peak, MaxOp{});
+    if (lane == 0)
         f.windows[w] = {power, peak};
 }
 
@@ -1219,14 +1235,17 @@ __device__ __forceinline__ short fadeSample(short value, int index, int count)
 // Fade, compaction and peak / audible range (tail.cu:240-297).  When the quality
 // gate or group volume is on, the same pass sums the mono power of the samples it
 // writes into the job's 250 ms body windows (measureBody, quality.cu:21-39): the
-// sums are integers, so the block partials and atomics give the reference's
-// totals in any order.
+// sums are integers, so the warp partials and atomics give the reference's
+// totals in any order.  A warp per 1024-frame block (eight per CTA), each lane
+// every 32nd frame; the reductions are warp shuffles, so no CTA barrier is needed.
 template <int Channels>
-__global__ void finalizeKernel(BatchView b, FinishView f, const short* input, int quality)
+__global__ void __launch_bounds__(kFinalizeWarps * 32) finalizeKernel(BatchView b, FinishView f, const short* input,
+                                                                      int quality)
 {
-    __shared__ int reduceI[32];
-    __shared__ unsigned long long reduceU[32];
-    const int block = int(blockIdx.x);
+    const int block = int(blockIdx.x) * kFinalizeWarps + int(threadIdx.x >> 5);
+    const int lane = int(threadIdx.x & 31);
+    if (block >= f.blockCount)
+        return;
     const int jobIndex = b.blockJob[block];
     const JobInfo job = b.jobs[jobIndex];
     cs_tail_result& result = f.results[jobIndex];
@@ -1253,7 +1272,7 @@ __global__ void finalizeKernel(BatchView b, FinishView f, const short* input, in
     unsigned long long powerA = 0, powerB = 0;
     int peak = 0, audibleFirst = frames, audibleLast = -1, clipped = 0;
     const int fadeStart = frames - fade;
-    for (int frame = first + int(threadIdx.x); frame < end; frame += blockDim.x) {
+    for (int frame = first + lane; frame < end; frame += 32) {
         int framePeak = 0, mono = 0;
         #pragma unroll
         for (int c = 0; c < Channels; ++c) {
@@ -1281,20 +1300,20 @@ __global__ void finalizeKernel(BatchView b, FinishView f, const short* input, in
                 powerB += power;
         }
     }
-    peak = blockReduce(peak, 0, MaxOp{}, reduceI);
-    audibleFirst = blockReduce(audibleFirst, frames, MinOp{}, reduceI);
-    audibleLast = blockReduce(audibleLast, -1, MaxOp{}, reduceI);
-    clipped = blockReduce(clipped, 0, SumOp{}, reduceI);
-    if (first < bodyEnd && paired) {          // uniform across the block
-        powerA = blockReduce(powerA, 0ull, SumOp{}, reduceU);
-        powerB = blockReduce(powerB, 0ull, SumOp{}, reduceU);
-        if (threadIdx.x == 0) {
+    peak = warpAll(peak, MaxOp{});
+    audibleFirst = warpAll(audibleFirst, MinOp{});
+    audibleLast = warpAll(audibleLast, MaxOp{});
+    clipped = warpAll(clipped, SumOp{});
+    if (first < bodyEnd && paired) {
+        powerA = warpAll(powerA, SumOp{});
+        powerB = warpAll(powerB, SumOp{});
+        if (lane == 0) {
             atomicAdd(f.bodyPower + bodyFirst + windowA, powerA);
             if (windowB != windowA)
                 atomicAdd(f.bodyPower + bodyFirst + windowB, powerB);
         }
     }
-    if (threadIdx.x == 0) {
+    if (lane == 0) {
         if (quality && clipped)
             atomicAdd(&result.audio.clipped, clipped);
         if (audibleLast >= 0) {
@@ -1453,7 +1472,8 @@ int launchFinish(const BatchView& b, const FinishView& f, bool natural, bool qua
         nativeResultKernel<<<jobGrid, threads, 0, stream>>>(b, f);
         ++launches;
         if (f.windowCount) {
-            quantizeMonoKernel<<<f.windowCount, 256, 0, stream>>>(b, f, tail.window);
+            quantizeMonoKernel<<<(f.windowCount + kFinalizeWarps - 1) / kFinalizeWarps, kFinalizeWarps * 32, 0,
+                                 stream>>>(b, f, tail.window);
             trimPowerKernel<<<windowGrid, threads, 0, stream>>>(b, f, tail, f.windowCount);
             trimLastKernel<<<windowGrid, threads, 0, stream>>>(b, f, tail, f.windowCount);
             launches += 3;
@@ -1465,9 +1485,11 @@ int launchFinish(const BatchView& b, const FinishView& f, bool natural, bool qua
     ++launches;
     if (f.blockCount) {
         if (natural)
-            finalizeKernel<1><<<f.blockCount, 128, 0, stream>>>(b, f, f.mono, quality ? 1 : 0);
+            finalizeKernel<1><<<(f.blockCount + kFinalizeWarps - 1) / kFinalizeWarps, kFinalizeWarps * 32, 0, stream>>>(
+                b, f, f.mono, quality ? 1 : 0);
         else
-            finalizeKernel<2><<<f.blockCount, 128, 0, stream>>>(b, f, static_cast<const short*>(b.mix),
+            finalizeKernel<2><<<(f.blockCount + kFinalizeWarps - 1) / kFinalizeWarps, kFinalizeWarps * 32, 0, stream>>>(
+                b, f, static_cast<const short*>(b.mix),
                                                               quality ? 1 : 0);
         ++launches;
     }

@@ -12,6 +12,7 @@
 #include "plan_blob.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <climits>
 #include <cmath>
 #include <cstdlib>
@@ -24,6 +25,7 @@
 #include <numeric>
 #include <stdexcept>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 namespace cs {
@@ -573,11 +575,27 @@ SharedPlan planSharedSources(const HostBatch& batch, size_t budgetBytes)
         uint64_t sample;
         double position, step, slope;
         int channels, sourceEnd, loopFirst, loopEnd, loopCrossfade;
-        bool operator<(const Key& o) const
+        bool operator==(const Key& o) const
         {
-            return std::tie(sample, position, step, slope, channels, sourceEnd, loopFirst, loopEnd, loopCrossfade) <
-                std::tie(o.sample, o.position, o.step, o.slope, o.channels, o.sourceEnd, o.loopFirst, o.loopEnd,
-                         o.loopCrossfade);
+            return sample == o.sample && position == o.position && step == o.step && slope == o.slope &&
+                channels == o.channels && sourceEnd == o.sourceEnd && loopFirst == o.loopFirst &&
+                loopEnd == o.loopEnd && loopCrossfade == o.loopCrossfade;
+        }
+    };
+    struct KeyHash {
+        size_t operator()(const Key& k) const
+        {
+            uint64_t h = 0x9e3779b97f4a7c15ull;
+            const auto mix = [&h](uint64_t v) { h = (h ^ v) * 0x100000001b3ull; h ^= h >> 29; };
+            uint64_t bits;
+            mix(k.sample);
+            std::memcpy(&bits, &k.position, 8); mix(bits);
+            std::memcpy(&bits, &k.step, 8); mix(bits);
+            std::memcpy(&bits, &k.slope, 8); mix(bits);
+            mix(uint64_t(uint32_t(k.channels)) << 32 | uint32_t(k.sourceEnd));
+            mix(uint64_t(uint32_t(k.loopFirst)) << 32 | uint32_t(k.loopEnd));
+            mix(uint64_t(uint32_t(k.loopCrossfade)));
+            return size_t(h);
         }
     };
     struct Entry {
@@ -586,7 +604,10 @@ SharedPlan planSharedSources(const HostBatch& batch, size_t budgetBytes)
     };
     SharedPlan plan;
     const size_t count = batch.voices.size();
-    std::map<Key, Entry> entries;
+    // Entries live in a deque (stable addresses); the map finds them by key.
+    std::deque<Entry> entryStore;
+    std::unordered_map<Key, Entry*, KeyHash> entries;
+    entries.reserve(count / 4 + 16);
     std::vector<const Entry*> entryOf(count, nullptr);
     for (size_t i = 0; i < count; ++i) {
         const cs_voice_span& v = batch.voices[i];
@@ -598,7 +619,12 @@ SharedPlan planSharedSources(const HostBatch& batch, size_t budgetBytes)
             frames = std::min(frames, silentFrom(v));
         const Key key{v.sample, v.position, v.step, v.pitchSlope, v.channels, v.sourceEnd, v.loopFirst, v.loopEnd,
                       v.loopCrossfade};
-        Entry& e = entries[key];
+        auto found = entries.find(key);
+        if (found == entries.end()) {
+            entryStore.emplace_back();
+            found = entries.emplace(key, &entryStore.back()).first;
+        }
+        Entry& e = *found->second;
         if (e.voice < 0)
             e.voice = int(i);
         e.frames = int(std::max<long long>(e.frames, frames));
@@ -608,16 +634,18 @@ SharedPlan planSharedSources(const HostBatch& batch, size_t budgetBytes)
     }
     // Sources played by more than one voice, the most voice frames saved first,
     // within the budget.
-    std::vector<const Entry*> chosen;
-    for (const auto& kv : entries)
-        if (kv.second.users > 1 && kv.second.frames > 0)
-            chosen.push_back(&kv.second);
+    // Candidates in order of first use (deterministic), then by the voice frames
+    // they save.
+    std::vector<Entry*> chosen;
+    for (Entry& e : entryStore)
+        if (e.users > 1 && e.frames > 0)
+            chosen.push_back(&e);
     std::stable_sort(chosen.begin(), chosen.end(), [](const Entry* a, const Entry* b) {
         return a->total - a->frames > b->total - b->frames;
     });
-    std::map<const Entry*, long long> offsetOf;
+    std::unordered_map<const Entry*, long long> offsetOf;
     size_t bytes = 0;
-    for (const Entry* e : chosen) {
+    for (Entry* e : chosen) {
         const int channels = batch.voices[size_t(e->voice)].channels;
         const size_t floats = alignFloats(size_t(e->frames) * size_t(channels));
         if ((plan.floats + floats) * sizeof(float) > budgetBytes)
@@ -731,6 +759,8 @@ struct cs_renderer {
     size_t bankCapacity = 0, uploaded = 0;
     size_t scratchLimit = 0;            // 0: derive from free memory
     bool sharedSources = true;          // render each shared voice source once per batch
+    // Host time spent staging batches, per phase (cs_renderer_host_ms).
+    double hostMs[cs::kHostPhases] = {};
     size_t peak = 0, waiting = 0, peakWaiting = 0, spilled = 0, downloaded = 0, cacheBudget = 0;
     size_t live = 0;                    // bytes of prepared batches alive
     void* hostPcm = nullptr;
@@ -779,6 +809,16 @@ struct cs_renderer {
 namespace cs {
 namespace {
 
+using HostClock = std::chrono::steady_clock;
+
+double msSince(HostClock::time_point& mark)
+{
+    const auto now = HostClock::now();
+    const double ms = std::chrono::duration<double, std::milli>(now - mark).count();
+    mark = now;
+    return ms;
+}
+
 size_t defaultScratchBudget()
 {
     size_t freeBytes = 0, total = 0;
@@ -813,7 +853,9 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     HostBatch& batch = p->batch;
     const bool assess = r.audio.enabled || r.groupMinimum > 0;
     const BodyGeometry body = bodyGeometry(r.audio);
+    auto mark = HostClock::now();
     batch.build(plans, count, r.tail.window, r.natural, assess, r.audio.enabled != 0, body, r.copies());
+    r.hostMs[0] += msSince(mark);
     p->assess = assess;
     if (assess && r.groupMinimum > 0) {
         // Volume groups: runs of equal nonzero ids (src/cuda/renderer.cpp:1751-1761).
@@ -830,8 +872,10 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     const size_t scratchBudget = r.scratchLimit ? r.scratchLimit : defaultScratchBudget();
     p->tables = planSegments(batch, scratchBudget);
     const SegmentTables& t = p->tables;
+    r.hostMs[1] += msSince(mark);
     if (r.sharedSources)
         p->shared = planSharedSources(batch, scratchBudget / 2);
+    r.hostMs[2] += msSince(mark);
     const SharedPlan& sh = p->shared;
     const size_t jobs = batch.jobs.size();
     const size_t frameBytes = r.natural ? sizeof(float2) : sizeof(short2);
@@ -998,6 +1042,7 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
                       reinterpret_cast<int2*>(base + oSharedTiles), lane.stream);
     check(cudaGetLastError(), "CUDA source tile expansion");
     check(cudaStreamSynchronize(lane.stream), "CUDA batch upload");
+    r.hostMs[3] += msSince(mark);
 
     BatchView& v = p->view;
     v.bank = r.bank;
@@ -2058,6 +2103,15 @@ int cs_renderer_set_scratch_limit(cs_renderer* r, size_t bytes)
             throw std::runtime_error("null renderer");
         r->scratchLimit = bytes;
     });
+}
+
+int cs_renderer_host_ms(const cs_renderer* r, double* ms, int capacity)
+{
+    if (!r || !ms)
+        return 0;
+    for (int i = 0; i < capacity && i < cs::kHostPhases; ++i)
+        ms[i] = r->hostMs[i];
+    return cs::kHostPhases;
 }
 
 int cs_renderer_set_shared_sources(cs_renderer* r, int enable)

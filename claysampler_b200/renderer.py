@@ -56,6 +56,7 @@ def library() -> ctypes.CDLL:
         lib.cs_prepared_destroy.argtypes = [vp]
         lib.cs_renderer_set_scratch_limit.argtypes = [vp, sz]
         lib.cs_renderer_set_shared_sources.argtypes = [vp, i32]
+        lib.cs_renderer_host_ms.argtypes = [vp, c.POINTER(c.c_double), i32]
         for name in ("cs_prepared_shared_sources", "cs_prepared_shared_frames"):
             getattr(lib, name).argtypes = [vp]
             getattr(lib, name).restype = sz
@@ -228,6 +229,13 @@ class Renderer:
 
     def set_scratch_limit(self, nbytes: int) -> None:
         _check(library().cs_renderer_set_scratch_limit(self.handle, nbytes))
+
+    def host_ms(self) -> dict[str, float]:
+        """Host milliseconds spent staging batches so far, per phase."""
+        out = (ctypes.c_double * 8)()
+        count = library().cs_renderer_host_ms(self.handle, out, 8)
+        names = ("index", "segments", "shared", "upload")
+        return {names[i] if i < len(names) else str(i): float(out[i]) for i in range(count)}
 
     def set_shared_sources(self, enable: bool) -> None:
         """Render each voice source shared by several voices once per batch (the
