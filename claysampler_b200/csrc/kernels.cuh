@@ -27,9 +27,10 @@ constexpr int kLeadTiers = CS_LEAD_TIERS; // tiers of long chains whose recurren
 // Moving-filter targets are stored per 32-frame chunk as three planes
 // (c0[32], c1[32], c2[32]) so the recurrence reads four frames per 128-bit load.
 constexpr int kRecChunkFrames = 32;
-// Host phases of staging a batch, timed per renderer: index building, segment
-// planning, shared-source planning, staging copies and upload.
-constexpr int kHostPhases = 4;
+// Host phases of staging a batch, timed per renderer: index building, scratch
+// budget, segment planning, shared-source planning, arena, staging pieces,
+// staging copies and upload issue, upload wait.
+constexpr int kHostPhases = 8;
 
 // A mix tile: kTileFrames frames of one job with the spans that overlap it
 // (the reference's Tile, src/cuda/render_types.h:70-74).

@@ -870,12 +870,13 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
         }
     }
     const size_t scratchBudget = r.scratchLimit ? r.scratchLimit : defaultScratchBudget();
+    r.hostMs[1] += msSince(mark);
     p->tables = planSegments(batch, scratchBudget);
     const SegmentTables& t = p->tables;
-    r.hostMs[1] += msSince(mark);
+    r.hostMs[2] += msSince(mark);
     if (r.sharedSources)
         p->shared = planSharedSources(batch, scratchBudget / 2);
-    r.hostMs[2] += msSince(mark);
+    r.hostMs[3] += msSince(mark);
     const SharedPlan& sh = p->shared;
     const size_t jobs = batch.jobs.size();
     const size_t frameBytes = r.natural ? sizeof(float2) : sizeof(short2);
@@ -957,6 +958,7 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
         r.live += p->arenaBytes;
     }
     r.record();
+    r.hostMs[4] += msSince(mark);
     auto* base = static_cast<unsigned char*>(p->arena);
     auto* staging = static_cast<unsigned char*>(cs_renderer::pinned(r.staging, r.stagingCapacity, uploadEnd));
     std::vector<CopyPiece> pieces;
@@ -1007,6 +1009,7 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     // workers copy the next slice.  Ranges are the staged pieces merged across small
     // gaps (section alignment); the direct uploads follow them in stream order, so
     // a merged range never leaves stale bytes over a directly uploaded piece.
+    r.hostMs[5] += msSince(mark);
     std::vector<std::pair<size_t, size_t>> ranges;
     for (const CopyPiece& piece : pieces) {
         const size_t a = size_t(static_cast<unsigned char*>(piece.dst) - staging), b = a + piece.bytes;
@@ -1041,8 +1044,9 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     launchExpandTiles(reinterpret_cast<const int4*>(base + oSharedRuns), int(sh.runs.size()),
                       reinterpret_cast<int2*>(base + oSharedTiles), lane.stream);
     check(cudaGetLastError(), "CUDA source tile expansion");
+    r.hostMs[6] += msSince(mark);
     check(cudaStreamSynchronize(lane.stream), "CUDA batch upload");
-    r.hostMs[3] += msSince(mark);
+    r.hostMs[7] += msSince(mark);
 
     BatchView& v = p->view;
     v.bank = r.bank;

@@ -5,7 +5,7 @@
 // Supported: RIFF/WAVE PCM 16/24/32-bit integer and 32-bit float, mono or stereo.
 // Integers scale by 2^-(bits-1) (exact in float32, as libsndfile's normalised
 // float read); a `smpl` chunk's first forward loop gives [start, end + 1).
-#include "host_types.hpp"
+#include "model.hpp"
 
 #include <cmath>
 #include <cstring>
@@ -14,7 +14,7 @@
 #include <limits>
 #include <stdexcept>
 
-namespace csh {
+namespace clayhost {
 namespace {
 
 uint32_t le32(const unsigned char* p) { return uint32_t(p[0]) | uint32_t(p[1]) << 8 | uint32_t(p[2]) << 16 | uint32_t(p[3]) << 24; }
@@ -153,4 +153,4 @@ void SampleBank::releaseDecoded()
         sample.offset = UINT64_MAX;
 }
 
-} // namespace csh
+} // namespace clayhost

@@ -1,7 +1,7 @@
 // C ABI of the host library (include/claysampler_host.h).
 #include "../../include/claysampler_host.h"
 #include "../csrc/plan_blob.hpp"
-#include "host_types.hpp"
+#include "model.hpp"
 
 #include <array>
 #include <climits>
@@ -70,8 +70,8 @@ void syncPath(const std::filesystem::path& path, int flags)
 } // namespace
 
 struct cs_host {
-    csh::SampleBank bank;
-    std::map<std::string, csh::Instrument> instruments;
+    clayhost::SampleBank bank;
+    std::map<std::string, clayhost::Instrument> instruments;
 };
 
 extern "C" {
@@ -97,15 +97,15 @@ int cs_host_plan(cs_host* host, const char* sfz, const char* midiPath, int rate,
     return guarded([&] {
         if (!host || !sfz || !midiPath || !image || !size)
             throw std::runtime_error("null argument");
-        const auto policy = tail == 0 ? csh::TailPolicy::natural : tail == 1 ? csh::TailPolicy::orig
-                                                                           : csh::TailPolicy::custom;
+        const auto policy = tail == 0 ? clayhost::TailPolicy::natural : tail == 1 ? clayhost::TailPolicy::orig
+                                                                                     : clayhost::TailPolicy::custom;
         auto instrument = host->instruments.find(sfz);
         if (instrument == host->instruments.end())
-            instrument = host->instruments.emplace(sfz, csh::loadInstrument(sfz, host->bank)).first;
-        const csh::Midi midi = csh::loadMidi(midiPath, rate, policy, groupVolume || quality);
-        const int musicEnd = midi.end + 1;
+            instrument = host->instruments.emplace(sfz, clayhost::readInstrument(sfz, host->bank)).first;
+        const clayhost::Score midi = clayhost::readScore(midiPath, rate, policy, groupVolume || quality);
+        const int musicEnd = midi.endFrame + 1;
         int limit = INT_MAX;
-        if (policy == csh::TailPolicy::natural) {
+        if (policy == clayhost::TailPolicy::natural) {
             limit = musicEnd + CS_NATURAL_TAIL_LIMIT_SECONDS * rate;
             if (maxAudio >= 0)
                 limit = std::min(limit, static_cast<int>(std::floor(maxAudio * rate)));
@@ -115,10 +115,10 @@ int cs_host_plan(cs_host* host, const char* sfz, const char* midiPath, int rate,
             limit = musicEnd + static_cast<int>(std::floor(tailMax * rate));
         }
         const int customFade = static_cast<int>(std::lround((tailFadeMs >= 0 ? tailFadeMs : 100) * (rate / 1000.)));
-        csh::Plan plan = csh::planRender(instrument->second, host->bank, midi, rate, 1, limit, policy);
+        clayhost::Plan plan = clayhost::planJob(instrument->second, host->bank, midi, rate, 1, limit, policy);
         plan.musicEnd = musicEnd;
         plan.limit = limit;
-        if (policy == csh::TailPolicy::custom && plan.tailClipped && plan.frames == limit)
+        if (policy == clayhost::TailPolicy::custom && plan.tailClipped && plan.frames == limit)
             plan.fadeFrames = std::min(customFade, std::max(0, plan.frames - musicEnd));
         plan.volumeGroup = group;
         plan.bodyFrames = midi.bodyFrames;
@@ -126,7 +126,7 @@ int cs_host_plan(cs_host* host, const char* sfz, const char* midiPath, int rate,
             plan.onsets = midi.onsets;
         std::vector<cs_control_point> points;
         std::vector<int64_t> offsets{0};
-        for (const auto& track : plan.controls) {
+        for (const auto& track : plan.tracks) {
             points.insert(points.end(), track.begin(), track.end());
             offsets.push_back(int64_t(points.size()));
         }
@@ -134,11 +134,11 @@ int cs_host_plan(cs_host* host, const char* sfz, const char* midiPath, int rate,
         view.spans = plan.spans.data();
         view.points = points.data();
         view.track_offsets = offsets.data();
-        view.modulation = plan.modulation.data();
+        view.modulation = plan.bindings.data();
         view.onsets = plan.onsets.data();
         view.span_count = int(plan.spans.size());
-        view.track_count = int(plan.controls.size());
-        view.modulation_count = int(plan.modulation.size());
+        view.track_count = int(plan.tracks.size());
+        view.modulation_count = int(plan.bindings.size());
         view.onset_count = int(plan.onsets.size());
         view.filter_tracks = plan.filterTracks;
         view.frames = plan.frames;
@@ -163,8 +163,8 @@ int cs_host_check_sfz(const char* sfz, int* regions)
     return guarded([&] {
         if (!sfz || !regions)
             throw std::runtime_error("null argument");
-        csh::SampleBank bank;
-        *regions = int(csh::loadInstrument(sfz, bank).regions.size());
+        clayhost::SampleBank bank;
+        *regions = int(clayhost::readInstrument(sfz, bank).regions.size());
     });
 }
 

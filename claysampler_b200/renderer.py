@@ -232,9 +232,9 @@ class Renderer:
 
     def host_ms(self) -> dict[str, float]:
         """Host milliseconds spent staging batches so far, per phase."""
-        out = (ctypes.c_double * 8)()
-        count = library().cs_renderer_host_ms(self.handle, out, 8)
-        names = ("index", "segments", "shared", "upload")
+        out = (ctypes.c_double * 16)()
+        count = library().cs_renderer_host_ms(self.handle, out, 16)
+        names = ("index", "budget", "segments", "shared", "arena", "pieces", "copy", "wait")
         return {names[i] if i < len(names) else str(i): float(out[i]) for i in range(count)}
 
     def set_shared_sources(self, enable: bool) -> None:

@@ -269,8 +269,8 @@ int cs_renderer_set_scratch_limit(cs_renderer* renderer, size_t bytes);
  * resamples every voice frame inline.  Applies to batches prepared afterwards. */
 int cs_renderer_set_shared_sources(cs_renderer* renderer, int enable);
 /* Host milliseconds the renderer spent staging batches so far, per phase: batch
- * index (voices, tiles, jobs), segment plan, shared-source plan, staging copies and
- * upload.  Writes up to `capacity` values and returns the phase count.  No
+ * index (voices, tiles, jobs), scratch budget, segment plan, shared-source plan,
+ * arena, staging pieces, staging copies and upload issue, upload wait.  Writes up to `capacity` values and returns the phase count.  No
  * counterpart in the reference. */
 int cs_renderer_host_ms(const cs_renderer* renderer, double* ms, int capacity);
 /* Shared sources of a prepared batch, the floats they hold, and the voice frames
