@@ -99,8 +99,10 @@ def parse():
                    help="jobs of 64 isolated notes of the 64-job batch's preset (80 % train, 20 % held out)")
     p.add_argument("--learned-mispredict", type=float, default=0.01,
                    help="mispredict rate the reservation margin is calibrated to on the training notes")
-    p.add_argument("--serve-jobs", type=int, default=200)
+    p.add_argument("--serve-jobs", type=int, default=3000, help="requests (3000 at 50/s: a minute of arrivals)")
     p.add_argument("--serve-rate", type=float, default=50.0)
+    p.add_argument("--serve-lanes", type=int, default=4, help="batches in flight (cs_renderer_set_lanes)")
+    p.add_argument("--serve-batch", type=int, default=32, help="jobs per batch at most")
     return p.parse_args()
 
 
@@ -620,7 +622,8 @@ def run_serve(args):
     torch.cuda.set_device(local)
     plans, arrivals, bank = serving_requests(args, rank)
     plans = [p.pin() for p in plans]
-    renderer = Renderer(device=local, natural=True, batch_jobs=64)
+    renderer = Renderer(device=local, natural=True, batch_jobs=args.serve_batch)
+    renderer.set_lanes(args.serve_lanes)
     renderer.upload_samples(bank)
     done = {}
 
@@ -654,8 +657,12 @@ def run_serve(args):
            "p99_ms": float(np.percentile(latency, 99)), "throughput_audio_s_per_s": audio / wall,
            "offered_audio_s_per_s": offered, "jobs": len(submitted), "rate_jobs_per_s": args.serve_rate,
            "wall_s": wall, "n_gpus": 1, "dtype": "f32", "data": "synthetic (seeded SFZ/WAV/MIDI)",
+           "deferred_launches": renderer.deferred_launches,
            "config": {"workload": "requests of the small kind over 8 presets, lengths log-uniform 5-300 s",
-                      "batch_jobs": 64, "lanes": 2}}
+                      "batch_jobs": args.serve_batch, "lanes": args.serve_lanes,
+                      "publication": "as batches finish (cs_poll)",
+                      "admission": "a batch launches while others run only if its estimated footprint fits in "
+                                   "half of the free device memory"}}
     if rank == 0:
         print(json.dumps(out))
     renderer.close()

@@ -626,18 +626,26 @@ __global__ void __launch_bounds__(kRecThreads, 1) recurrenceKernel(BatchView b, 
                      tgtBytes, &bars[local][slot]);
     };
     uint32_t phases = 0;                 // bit k: parity of buffer k's next completion
+    uint32_t inflight = 0;               // bit k: buffer k has a copy issued and not yet waited for
     for (int slot = 0; slot < kRecBuffers && next.span >= 0; ++slot) {
         if (leader)
             issue(slot);
+        inflight |= 1u << slot;
         advanceRun(b, s, next, fslot);
     }
     int slot = 0;
     while (consume.span >= 0) {
         if (!barrierWait(&bars[local][slot], (phases >> slot) & 1u)) {
+            // Give up: flag the batch, issue nothing more, and wait (bounded) for
+            // the copies still in flight into this chain's buffers before leaving.
             atomicExch(error, 1);
+            for (int k = 0; k < kRecBuffers; ++k)
+                if (inflight >> k & 1u)
+                    barrierWait(&bars[local][k], (phases >> k) & 1u);
             return;
         }
         phases ^= 1u << slot;
+        inflight &= ~(1u << slot);
         const int count = min(kRecChunk, consume.stop - consume.pos);
         const int rel = consume.pos - consume.start;
         const int sections = consume.sections;
@@ -684,6 +692,7 @@ __global__ void __launch_bounds__(kRecThreads, 1) recurrenceKernel(BatchView b, 
         if (next.span >= 0) {
             if (leader)
                 issue(slot);
+            inflight |= 1u << slot;
             advanceRun(b, s, next, fslot);
         }
         slot = slot + 1 == kRecBuffers ? 0 : slot + 1;
@@ -928,6 +937,146 @@ __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(Ba
             }
         } else {
             static_cast<short2*>(b.mix)[job.offset + frame] = make_short2(toPcm16(x), toPcm16(y));
+        }
+    }
+    if (Natural) {
+        power = blockReduce(power, 0.0, SumOp{}, reduceD);
+        peak = blockReduce(peak, 0.f, MaxOp{}, reduceF);
+        if (threadIdx.x == 0)
+            stats[block] = {power, peak};
+    }
+}
+
+// The mix of batches whose mix kernel resamples no voice itself (every
+// unfiltered voice reads a shared source, or every voice is filtered).  A CTA per
+// 1024-frame tail block; the 64 threads of each 256-frame tile take four of its
+// frames each, 64 apart (so every warp access stays coalesced), and walk the
+// tile's voices once for all four: a voice's fields are read once per four frames
+// and its four frames are in flight together.  Each frame still adds its voices
+// in span order (renderTiles, render.cu:458-523), so the sums are those of the
+// frame-per-thread mix; the block power and peak are reduced in the same pass
+// (scanStereo, tail.cu:54-81).
+constexpr int kFramesPerThread = kTilesPerBlock;           // 4
+constexpr int kTileThreads = kTileFrames / kFramesPerThread;
+
+template <bool Natural>
+__global__ void __launch_bounds__(kMixThreads, 4) mixSharedKernel(BatchView b, SegmentView s, StereoStats* stats)
+{
+    __shared__ double reduceD[32];
+    __shared__ float reduceF[32];
+    __shared__ MixVoice staged[kTilesPerBlock][kMixStaged];
+    __shared__ MixTile tiles[kTilesPerBlock];
+    const int block = s.blocks[blockIdx.x];
+    const int jobIndex = b.blockJob[block];
+    const JobInfo job = b.jobs[jobIndex];
+    const int local = block - job.blockFirst;
+    const int jobTiles = (job.frames + kTileFrames - 1) / kTileFrames;
+    {
+        const int k = int(threadIdx.x) / kMixStaged, i = int(threadIdx.x) % kMixStaged;
+        const int tileIndex = local * kTilesPerBlock + k;
+        const MixTile tile = tileIndex < jobTiles ? b.tiles[job.tileFirst + tileIndex] : MixTile{0, 0};
+        if (i == 0)
+            tiles[k] = tile;
+        if (i < tile.count && tile.count <= kMixStaged)
+            staged[k][i] = mixVoiceOf(b, s, __ldg(b.indices + tile.first + i));
+    }
+    __syncthreads();
+    const int k = int(threadIdx.x) / kTileThreads, i = int(threadIdx.x) % kTileThreads;
+    const MixTile tile = tiles[k];
+    const int base = local * kBlockFrames + k * kTileFrames + i;
+    int frame[kFramesPerThread];
+    bool live[kFramesPerThread];
+    float pan[kFramesPerThread], left[kFramesPerThread], right[kFramesPerThread];
+    float wetLeft[kFramesPerThread], wetRight[kFramesPerThread];
+    bool any = false;
+    #pragma unroll
+    for (int j = 0; j < kFramesPerThread; ++j) {
+        frame[j] = base + j * kTileThreads;
+        live[j] = frame[j] < job.frames && frame[j] >= s.first && frame[j] < s.end;
+        any |= live[j];
+        pan[j] = live[j] ? trackAt(b.points, job.tracks[2], job.tracks[3], frame[j]) : 0.f;
+        left[j] = right[j] = wetLeft[j] = wetRight[j] = 0.f;
+    }
+    for (int n = 0; any && n < tile.count; ++n) {
+        const MixVoice m = tile.count <= kMixStaged ? staged[k][n] : mixVoiceOf(b, s, __ldg(b.indices + tile.first + n));
+        bool in[kFramesPerThread];
+        bool touched = false;
+        #pragma unroll
+        for (int j = 0; j < kFramesPerThread; ++j) {
+            in[j] = live[j] && frame[j] >= m.begin && frame[j] < m.end;
+            touched |= in[j];
+        }
+        if (!touched)
+            continue;
+        if (m.kind == 1) {
+            #pragma unroll
+            for (int j = 0; j < kFramesPerThread; ++j)
+                if (in[j]) {
+                    const float2 x = *reinterpret_cast<const float2*>(b.filtered + (m.offset + 2ll * frame[j]));
+                    wetLeft[j] += x.x;
+                    wetRight[j] += x.y;
+                }
+        } else if (m.kind == 2) {
+            // Mono filtered voices are panned after the filter.
+            const cs_voice_span& v = b.voices[m.index];
+            #pragma unroll
+            for (int j = 0; j < kFramesPerThread; ++j)
+                if (in[j]) {
+                    const float x = b.filtered[m.offset + frame[j]];
+                    float offset = pan[j];
+                    for (int q = v.firstModulation; q < v.firstModulation + v.modulationCount; ++q) {
+                        const cs_voice_modulation mod = b.modulation[q];
+                        if (mod.target == CS_MOD_PAN)
+                            offset += bindingAt(mod, b.points, frame[j]);
+                    }
+                    const float2 gains = panGains(v, offset);
+                    wetLeft[j] += x * gains.x;
+                    wetRight[j] += x * gains.y;
+                }
+        } else if (m.kind >= 3) {
+            // voiceFrame with the source read from the shared sources.
+            const cs_voice_span& v = b.voices[m.index];
+            #pragma unroll
+            for (int j = 0; j < kFramesPerThread; ++j) {
+                if (!in[j])
+                    continue;
+                const float level = envelopeAt(v, frame[j]);
+                if (level <= 0)
+                    continue;
+                const VoiceMods mods = voiceMods(v, b.points, b.modulation, level, pan[j], frame[j]);
+                float2 source = make_float2(0.f, 0.f);
+                if (frame[j] < m.sharedEnd) {
+                    if (m.kind == 3) {
+                        const float x = __ldg(b.shared + (m.offset + frame[j]));
+                        source = make_float2(x, x);
+                    } else {
+                        source = __ldg(reinterpret_cast<const float2*>(b.shared + (m.offset + 2ll * frame[j])));
+                    }
+                }
+                const float2 out = voiceOutputFrom(source, v, mods, false);
+                left[j] += out.x;
+                right[j] += out.y;
+            }
+        }
+    }
+    double power = 0;
+    float peak = 0;
+    #pragma unroll
+    for (int j = 0; j < kFramesPerThread; ++j) {
+        if (!live[j])
+            continue;
+        const float amplitude = jobGainAt(b.points, job.tracks, frame[j]);
+        const float x = fmaf(left[j], amplitude, wetLeft[j]), y = fmaf(right[j], amplitude, wetRight[j]);
+        if (Natural) {
+            static_cast<float2*>(b.mix)[job.offset + frame[j]] = make_float2(x, y);
+            if (!isfinite(x) || !isfinite(y)) {
+                peak = __int_as_float(0x7f800000);
+            } else {
+                peak = fmaxf(peak, fmaxf(fabsf(x), fabsf(y)));
+                power += double(__fmul_rn(x, x)) + double(__fmul_rn(y, y));
+            }
+        } else {
+            static_cast<short2*>(b.mix)[job.offset + frame[j]] = make_short2(toPcm16(x), toPcm16(y));
         }
     }
     if (Natural) {
@@ -1443,13 +1592,15 @@ void launchMix(const BatchView& b, const SegmentView& s, bool natural, StereoSta
                                                     kInlineMixCarveout)});
         });
     const auto launch = [&](auto kernel) { kernel<<<s.blockCount, kMixThreads, 0, stream>>>(b, s, stats); };
-    switch ((natural ? 3 : 0) + b.inlineVoices) {
-    case 0: launch(mixKernel<false, 0>); break;
-    case 1: launch(mixKernel<false, 1>); break;
-    case 2: launch(mixKernel<false, 2>); break;
-    case 3: launch(mixKernel<true, 0>); break;
-    case 4: launch(mixKernel<true, 1>); break;
-    default: launch(mixKernel<true, 2>); break;
+    if (b.inlineVoices == 1) {
+        if (natural)
+            launch(mixKernel<true, 1>);
+        else
+            launch(mixKernel<false, 1>);
+    } else if (natural) {
+        launch(mixSharedKernel<true>);
+    } else {
+        launch(mixSharedKernel<false>);
     }
 }
 

@@ -751,14 +751,21 @@ struct cs_renderer {
         size_t arenaCapacity = 0;
         void* download = nullptr;       // page-locked: the lane's published batch
         size_t downloadCapacity = 0;
+        void* staging = nullptr;        // page-locked: the lane's batch uploads
+        size_t stagingCapacity = 0;
+        cudaEvent_t uploaded = nullptr; // the lane's last uploads have been read
     };
-    static constexpr int kLanes = 2;
+    static constexpr int kLanes = 4;
     Lane lanes[kLanes];
+    int laneCount = 2;                  // batches in flight at most (cs_renderer_set_lanes)
     float* sinc = nullptr;
     float* bank = nullptr;
     size_t bankCapacity = 0, uploaded = 0;
     size_t scratchLimit = 0;            // 0: derive from free memory
     bool sharedSources = true;          // render each shared voice source once per batch
+    size_t budgetCache = 0;             // derived scratch budget of the current render call (0: stale)
+    size_t deferred = 0;                // serving: launches deferred for lack of free memory
+    std::string error;                  // message of this renderer's last failed call
     // Host time spent staging batches, per phase (cs_renderer_host_ms).
     double hostMs[cs::kHostPhases] = {};
     size_t peak = 0, waiting = 0, peakWaiting = 0, spilled = 0, downloaded = 0, cacheBudget = 0;
@@ -869,7 +876,10 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
             p->groups.push_back(make_int2(int(first), int(end)));
         }
     }
-    const size_t scratchBudget = r.scratchLimit ? r.scratchLimit : defaultScratchBudget();
+    // The derived budget is read once per render call (cudaMemGetInfo is slow).
+    if (!r.scratchLimit && !r.budgetCache)
+        r.budgetCache = defaultScratchBudget();
+    const size_t scratchBudget = r.scratchLimit ? r.scratchLimit : r.budgetCache;
     r.hostMs[1] += msSince(mark);
     p->tables = planSegments(batch, scratchBudget);
     const SegmentTables& t = p->tables;
@@ -960,7 +970,12 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     r.record();
     r.hostMs[4] += msSince(mark);
     auto* base = static_cast<unsigned char*>(p->arena);
-    auto* staging = static_cast<unsigned char*>(cs_renderer::pinned(r.staging, r.stagingCapacity, uploadEnd));
+    // Render-window batches stage through their lane's buffer, reused once the
+    // lane's previous uploads have been read; other batches use the renderer's.
+    if (shared && lane.uploaded)
+        check(cudaEventSynchronize(lane.uploaded), "CUDA staging reuse");
+    auto* staging = static_cast<unsigned char*>(shared ? cs_renderer::pinned(lane.staging, lane.stagingCapacity, uploadEnd)
+                                                       : cs_renderer::pinned(r.staging, r.stagingCapacity, uploadEnd));
     std::vector<CopyPiece> pieces;
     const auto stage = [&](size_t offset, const auto& items) {
         if (!items.empty())
@@ -976,7 +991,9 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
             const size_t bytes = count * sizeof(cs_control_point);
             if (!bytes)
                 continue;
-            if (pageLocked(first))
+            // Large page-locked arrays go up directly; small ones are cheaper to copy
+            // into the staging buffer than to upload one by one.
+            if (bytes >= (size_t(256) << 10) && pageLocked(first))
                 direct.push_back({base + at, first, bytes});
             else
                 pieces.push_back({staging + at, first, bytes});
@@ -1045,7 +1062,15 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
                       reinterpret_cast<int2*>(base + oSharedTiles), lane.stream);
     check(cudaGetLastError(), "CUDA source tile expansion");
     r.hostMs[6] += msSince(mark);
-    check(cudaStreamSynchronize(lane.stream), "CUDA batch upload");
+    if (shared) {
+        // The batch runs on the lane's stream after its uploads; the staging buffer
+        // is reused once this event has passed.
+        if (!lane.uploaded)
+            check(cudaEventCreateWithFlags(&lane.uploaded, cudaEventDisableTiming), "CUDA upload event");
+        check(cudaEventRecord(lane.uploaded, lane.stream), "CUDA upload event");
+    } else {
+        check(cudaStreamSynchronize(lane.stream), "CUDA batch upload");
+    }
     r.hostMs[7] += msSince(mark);
 
     BatchView& v = p->view;
@@ -1314,6 +1339,10 @@ int guarded(F&& body)
     }
 }
 
+// As guarded, and the message is also kept on the renderer (cs_renderer_last_error).
+template <class F>
+int guardedOn(cs_renderer* r, F&& body);
+
 
 // Renderer::renderWindow (src/cuda/renderer.cpp:1748-1820) over staged batches.
 // Batches take up to batchJobs plans and never cut a volume group unless the group
@@ -1334,6 +1363,7 @@ public:
 
     void render(const cs_plan* plans, size_t count)
     {
+        r.budgetCache = 0;
         queue.assign(plans, plans + count);
         next = 0;
         for (;;) {
@@ -1348,9 +1378,10 @@ public:
     // ticket (queue position) of the first plan.
     size_t submit(const cs_plan* plans, size_t count)
     {
-        const size_t ticket = queue.size();
+        const size_t ticket = ticketBase + queue.size();
+        r.budgetCache = 0;
         queue.insert(queue.end(), plans, plans + count);
-        launch(false);
+        launch(false, true);
         return ticket;
     }
 
@@ -1362,19 +1393,53 @@ public:
         publish = fn;
         user = data;
         size_t published = 0;
-        while (!flight.empty()) {
-            const cudaError_t state = cudaEventQuery(flight.front().batch->end);
-            if (state != cudaSuccess && state != cudaErrorNotReady)
-                check(state, "CUDA batch completion");
-            if (state == cudaErrorNotReady && !wait)
-                break;
-            published += flight.front().batch->batch.jobs.size();
-            publishFront();
-            launch(false);
+        // Every finished batch is published, in the order they finish (a short
+        // job's batch does not wait for an older, longer one); with `wait`, the
+        // oldest is waited for when none has finished.
+        for (;;) {
+            auto done = flight.end();
+            for (auto f = flight.begin(); f != flight.end(); ++f) {
+                const cudaError_t state = cudaEventQuery(f->batch->copied ? f->batch->copied : f->batch->end);
+                if (state != cudaSuccess && state != cudaErrorNotReady)
+                    check(state, "CUDA batch completion");
+                if (state == cudaSuccess) {
+                    done = f;
+                    break;
+                }
+            }
+            if (done == flight.end()) {
+                if (!wait || flight.empty())
+                    break;
+                done = flight.begin();
+            }
             wait = false;                       // one blocking wait per call at most
+            InFlight item = *done;
+            flight.erase(done);
+            published += item.batch->batch.jobs.size();
+            std::unique_ptr<cs_prepared, void (*)(cs_prepared*)> guard(item.batch, cs_prepared_destroy);
+            publishBatch(*item.batch, item.first);
+            guard.reset();
+            launch(false, true);
         }
-        launch(false);
+        launch(false, true);
+        dropPublished();
         return published;
+    }
+
+    // Serving: forget the queued plans every batch has taken, keeping tickets
+    // (queue positions) stable through a base offset.
+    void dropPublished()
+    {
+        size_t oldest = next;
+        for (const InFlight& f : flight)
+            oldest = std::min(oldest, f.first);
+        if (oldest < 4096 || oldest < queue.size() / 2 || !chunks.empty())
+            return;
+        queue.erase(queue.begin(), queue.begin() + std::ptrdiff_t(oldest));
+        for (InFlight& f : flight)
+            f.first -= oldest;
+        next -= oldest;
+        ticketBase += oldest;
     }
 
     size_t pending() const { return queue.size() - next; }
@@ -1389,23 +1454,40 @@ public:
 
 private:
     size_t next = 0;                            // first queued plan not yet launched
+    size_t ticketBase = 0;                      // tickets of the plans dropped from the queue
 
-    // Keeps up to kLanes batches in flight: the next batch is staged and launched
-    // on a free lane while the others run (batches are published in order).
-    // `mayRefill`: ask the refill callback for more plans when the queue runs dry.
-    void launch(bool mayRefill)
+    // Keeps up to laneCount batches in flight: the next batch is staged and
+    // launched on a free lane while the others run.  `mayRefill`: ask the refill
+    // callback for more plans when the queue runs dry.  `admit`: while batches are
+    // in flight, launch another only if its estimated device footprint fits in half
+    // of the free device memory (the reference's admission of resident jobs,
+    // src/cuda/renderer.cpp:1447-1481).
+    void launch(bool mayRefill, bool admit = false)
     {
-        while (flight.size() < size_t(cs_renderer::kLanes)) {
+        size_t freeBytes = 0;
+        bool freeKnown = false;
+        while (flight.size() < size_t(std::clamp(r.laneCount, 1, cs_renderer::kLanes))) {
             if (next == queue.size() && !(mayRefill && more(flight.empty())))
                 break;
             size_t jobs = batchEnd(next, std::min(queue.size(), next + r.batchJobs)) - next;
+            if (admit && !flight.empty()) {
+                if (!freeKnown) {
+                    size_t total = 0;
+                    check(cudaMemGetInfo(&freeBytes, &total), "CUDA free memory");
+                    freeKnown = true;
+                }
+                if (footprint(next, jobs) > freeBytes / 2) {
+                    ++r.deferred;
+                    break;
+                }
+            }
             if (splitGroup(next, jobs)) {
                 // Chunks of a volume group larger than a batch go one at a time.
                 drain();
                 next = renderAlone(next, jobs);
                 continue;
             }
-            const int lane = flight.empty() ? 0 : 1 - flight.front().batch->lane;
+            const int lane = freeLane();
             cs_prepared* prepared = tryPrepare(next, jobs, lane);
             if (!prepared) {
                 drain();
@@ -1422,7 +1504,33 @@ private:
             enqueueDownload(r, *prepared);
             flight.push_back({prepared, next});
             next += jobs;
+            freeKnown = false;
         }
+    }
+
+    int freeLane() const
+    {
+        for (int lane = 0; lane < cs_renderer::kLanes; ++lane) {
+            bool busy = false;
+            for (const InFlight& f : flight)
+                busy |= f.batch->lane == lane;
+            if (!busy)
+                return lane;
+        }
+        return 0;
+    }
+
+    // Device bytes a batch of `jobs` queued plans needs, estimated from its frames
+    // and spans: the float mix, mono and packed PCM, tail statistics and the span
+    // records (the arena's large sections).
+    size_t footprint(size_t first, size_t jobs) const
+    {
+        size_t frames = 0, spans = 0;
+        for (size_t j = first; j < first + jobs; ++j) {
+            frames += size_t(queue[j].frames);
+            spans += size_t(queue[j].span_count);
+        }
+        return frames * (sizeof(float2) + 3 * sizeof(short)) + spans * (sizeof(cs_voice_span) + sizeof(ChainState));
     }
 
 private:
@@ -1477,6 +1585,7 @@ private:
             } catch (const CudaError& e) {
                 if (e.code != cudaErrorMemoryAllocation)
                     throw;
+                r.budgetCache = 0;
                 bool released = false;
                 if (!flight.empty()) {
                     drain();
@@ -1594,7 +1703,7 @@ private:
     {
         cs_batch rejected{};
         rejected.failed_scratch_bytes = 1;
-        publish(user, &rejected, first);
+        publish(user, &rejected, ticketBase + first);
     }
 
     void deliver(const int16_t* pcm, size_t samples, const cs_tail_result* results, size_t count, double kernel,
@@ -1607,7 +1716,7 @@ private:
         batch.results = results;
         batch.result_count = count;
         batch.kernel_seconds = kernel;
-        publish(user, &batch, first);
+        publish(user, &batch, ticketBase + first);
     }
 
     int16_t* hostPcm(size_t samples)
@@ -1805,9 +1914,23 @@ private:
 } // namespace
 } // namespace cs
 
+namespace cs {
+namespace {
+template <class F>
+int guardedOn(cs_renderer* r, F&& body)
+{
+    const int status = guarded(std::forward<F>(body));
+    if (status && r)
+        r->error = lastError;
+    return status;
+}
+} // namespace
+} // namespace cs
+
 extern "C" {
 
 const char* cs_last_error(void) { return cs::lastError.c_str(); }
+const char* cs_renderer_last_error(const cs_renderer* r) { return r ? r->error.c_str() : ""; }
 
 int cs_renderer_create(int device, int natural, const cs_audio_config* audio, int group_minimum,
                        size_t waiting_limit, size_t batch_jobs, cs_renderer** out)
@@ -1882,8 +2005,11 @@ void cs_renderer_destroy(cs_renderer* r)
     }
     if (r->hostPcm) cudaFreeHost(r->hostPcm);
     if (r->staging) cudaFreeHost(r->staging);
-    for (auto& lane : r->lanes)
+    for (auto& lane : r->lanes) {
         if (lane.download) cudaFreeHost(lane.download);
+        if (lane.staging) cudaFreeHost(lane.staging);
+        if (lane.uploaded) cudaEventDestroy(lane.uploaded);
+    }
     for (auto& lane : r->lanes) {
         if (lane.stream) cudaStreamDestroy(lane.stream);
         for (int k = 0; k < cs::kLeadTiers; ++k) {
@@ -1897,7 +2023,7 @@ void cs_renderer_destroy(cs_renderer* r)
 
 int cs_upload_samples(cs_renderer* r, const float* pcm, size_t floats, int fresh)
 {
-    return cs::guarded([&] {
+    return cs::guardedOn(r, [&] {
         if (!r)
             throw std::runtime_error("null renderer");
         cs::check(cudaSetDevice(r->device), "CUDA device");
@@ -1927,7 +2053,7 @@ int cs_upload_samples(cs_renderer* r, const float* pcm, size_t floats, int fresh
 
 int cs_prepare(cs_renderer* r, const cs_plan* plans, size_t count, cs_prepared** out)
 {
-    return cs::guarded([&] {
+    return cs::guardedOn(r, [&] {
         if (!r || !out)
             throw std::runtime_error("null renderer or output handle");
         cs::checkPlans(plans, count);
@@ -1937,7 +2063,7 @@ int cs_prepare(cs_renderer* r, const cs_plan* plans, size_t count, cs_prepared**
 
 int cs_run(cs_renderer* r, cs_prepared* p, void* stream)
 {
-    return cs::guarded([&] {
+    return cs::guardedOn(r, [&] {
         if (!r || !p)
             throw std::runtime_error("null renderer or batch");
         if (!r->bank && !p->batch.voices.empty())
@@ -1949,7 +2075,7 @@ int cs_run(cs_renderer* r, cs_prepared* p, void* stream)
 int cs_collect(cs_renderer* r, cs_prepared* p, int16_t* pcm, size_t capacity, size_t* samples,
                cs_tail_result* results)
 {
-    return cs::guarded([&] {
+    return cs::guardedOn(r, [&] {
         if (!r || !p || !p->ran)
             throw std::runtime_error("batch has not been run");
         const size_t count = cs::collectResults(*r, *p);
@@ -1970,7 +2096,7 @@ int cs_collect(cs_renderer* r, cs_prepared* p, int16_t* pcm, size_t capacity, si
 
 int cs_copy_mix(cs_renderer* r, cs_prepared* p, void* host, size_t bytes)
 {
-    return cs::guarded([&] {
+    return cs::guardedOn(r, [&] {
         if (!r || !p || !p->ran)
             throw std::runtime_error("batch has not been run");
         if (bytes < p->mixBytes)
@@ -2047,7 +2173,7 @@ void cs_prepared_destroy(cs_prepared* p)
 int cs_render_window(cs_renderer* r, const cs_plan* plans, size_t count, cs_publish_fn publish,
                      cs_refill_fn refill, void* user)
 {
-    return cs::guarded([&] {
+    return cs::guardedOn(r, [&] {
         if (!r || !publish)
             throw std::runtime_error("null renderer or publish callback");
         cs::checkPlans(plans, count);
@@ -2059,7 +2185,7 @@ int cs_render_window(cs_renderer* r, const cs_plan* plans, size_t count, cs_publ
 
 int cs_submit(cs_renderer* r, const cs_plan* plans, size_t count, uint64_t* first_ticket)
 {
-    return cs::guarded([&] {
+    return cs::guardedOn(r, [&] {
         if (!r)
             throw std::runtime_error("null renderer");
         cs::checkPlans(plans, count);
@@ -2073,7 +2199,7 @@ int cs_submit(cs_renderer* r, const cs_plan* plans, size_t count, uint64_t* firs
 
 int cs_poll(cs_renderer* r, int wait, cs_publish_fn publish, void* user, size_t* published)
 {
-    return cs::guarded([&] {
+    return cs::guardedOn(r, [&] {
         if (!r || !publish)
             throw std::runtime_error("null renderer or publish callback");
         const size_t count = r->service ? r->service->poll(wait != 0, publish, user) : 0;
@@ -2102,12 +2228,25 @@ size_t cs_downloaded_bytes(const cs_renderer* r) { return r ? r->downloaded : 0;
 // exercises segmentation with a special build that limits scratch to 64 KiB.
 int cs_renderer_set_scratch_limit(cs_renderer* r, size_t bytes)
 {
-    return cs::guarded([&] {
+    return cs::guardedOn(r, [&] {
         if (!r)
             throw std::runtime_error("null renderer");
         r->scratchLimit = bytes;
     });
 }
+
+int cs_renderer_set_lanes(cs_renderer* r, int lanes)
+{
+    return cs::guardedOn(r, [&] {
+        if (!r)
+            throw std::runtime_error("null renderer");
+        if (lanes < 1 || lanes > cs_renderer::kLanes)
+            throw std::runtime_error("lanes must be 1 to " + std::to_string(cs_renderer::kLanes));
+        r->laneCount = lanes;
+    });
+}
+
+size_t cs_renderer_deferred_launches(const cs_renderer* r) { return r ? r->deferred : 0; }
 
 int cs_renderer_host_ms(const cs_renderer* r, double* ms, int capacity)
 {
@@ -2120,7 +2259,7 @@ int cs_renderer_host_ms(const cs_renderer* r, double* ms, int capacity)
 
 int cs_renderer_set_shared_sources(cs_renderer* r, int enable)
 {
-    return cs::guarded([&] {
+    return cs::guardedOn(r, [&] {
         if (!r)
             throw std::runtime_error("null renderer");
         r->sharedSources = enable != 0;

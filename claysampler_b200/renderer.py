@@ -57,6 +57,9 @@ def library() -> ctypes.CDLL:
         lib.cs_renderer_set_scratch_limit.argtypes = [vp, sz]
         lib.cs_renderer_set_shared_sources.argtypes = [vp, i32]
         lib.cs_renderer_host_ms.argtypes = [vp, c.POINTER(c.c_double), i32]
+        lib.cs_renderer_set_lanes.argtypes = [vp, i32]
+        lib.cs_renderer_deferred_launches.argtypes = [vp]
+        lib.cs_renderer_deferred_launches.restype = sz
         for name in ("cs_prepared_shared_sources", "cs_prepared_shared_frames"):
             getattr(lib, name).argtypes = [vp]
             getattr(lib, name).restype = sz
@@ -229,6 +232,14 @@ class Renderer:
 
     def set_scratch_limit(self, nbytes: int) -> None:
         _check(library().cs_renderer_set_scratch_limit(self.handle, nbytes))
+
+    def set_lanes(self, lanes: int) -> None:
+        """Batches in flight at most (1-4); submit / poll publishes them as they finish."""
+        _check(library().cs_renderer_set_lanes(self.handle, lanes))
+
+    @property
+    def deferred_launches(self) -> int:
+        return int(library().cs_renderer_deferred_launches(self.handle))
 
     def host_ms(self) -> dict[str, float]:
         """Host milliseconds spent staging batches so far, per phase."""

@@ -216,6 +216,10 @@ size_t cs_downloaded_bytes(const cs_renderer* renderer);
 
 /* Message of the last failed call on this thread (no reference counterpart: the
  * reference reports failures as C++ exceptions). */
+/* The message of the last failed call on this renderer (empty when none): the
+ * reference's exception text for that renderer, where cs_last_error is the calling
+ * thread's. */
+const char* cs_renderer_last_error(const cs_renderer* renderer);
 const char* cs_last_error(void);
 
 /* ---- staged batches (measurement and tests; no reference counterpart) -----------
@@ -273,6 +277,14 @@ int cs_renderer_set_shared_sources(cs_renderer* renderer, int enable);
  * arena, staging pieces, staging copies and upload issue, upload wait.  Writes up to `capacity` values and returns the phase count.  No
  * counterpart in the reference. */
 int cs_renderer_host_ms(const cs_renderer* renderer, double* ms, int capacity);
+/* Batches in flight at most (1-4, default 2), each on its own stream lane with its
+ * own arena.  cs_render_window publishes batches in order; cs_poll publishes them
+ * as they finish.  The reference keeps one rolling batch of resident jobs
+ * (src/cuda/renderer.cpp:1353-1746). */
+int cs_renderer_set_lanes(cs_renderer* renderer, int lanes);
+/* Serving: how often a batch launch waited because its estimated footprint
+ * exceeded half of the free device memory while other batches were in flight. */
+size_t cs_renderer_deferred_launches(const cs_renderer* renderer);
 /* Shared sources of a prepared batch, the floats they hold, and the voice frames
  * that read them instead of resampling. */
 size_t cs_prepared_shared_sources(const cs_prepared* prepared);

@@ -1,7 +1,8 @@
 """Serving: non-blocking submission with continuous batching (cs_submit /
 cs_poll).  Jobs submitted while others are on the GPU are admitted as stream lanes
-free up, published in ticket order, and each job's audio and results are the same
-as when it is rendered alone."""
+free up (and device memory allows), each batch is published as it finishes under
+its jobs' tickets, and each job's audio and results are the same as when it is
+rendered alone."""
 import numpy as np
 import pytest
 
@@ -32,6 +33,7 @@ def test_submissions_while_rendering_match_jobs_alone(ref_session, batch_mini, p
     plans += [ref_session.plan(j.sfz, j.midi) for j in batch_mini]          # repeats in other batches
     bank = ref_session.bank()
     renderer = Renderer(natural=True, batch_jobs=2)
+    renderer.set_lanes(3)
     renderer.upload_samples(bank)
     published = {}
     order = []
@@ -50,7 +52,8 @@ def test_submissions_while_rendering_match_jobs_alone(ref_session, batch_mini, p
     while renderer.pending_jobs:
         renderer.poll(publish, wait=True)
     assert tickets == [0, 3, 5]
-    assert sorted(published) == list(range(len(plans))) and order == sorted(order)
+    # Every ticket once; batches may finish (and publish) out of ticket order.
+    assert sorted(published) == list(range(len(plans))) and len(order) == len(set(order))
     for ticket, plan in enumerate(plans):
         pcm, result = alone(renderer, plan)
         got_pcm, got_result = published[ticket]
