@@ -117,6 +117,120 @@ __global__ void __launch_bounds__(kSamples) forwardKernel(const float* __restric
     y[2 * size_t(i) + 1] = fmaf(out1, s.targetStd[1], s.targetMean[1]);
 }
 
+// ---- inference on the tensor cores --------------------------------------------------
+//
+// A warp takes 16 samples.  Layer 1 (16 -> 64) and layer 2 (64 -> 64) run as
+// mma.sync m16n8k16 with BF16 operands and FP32 accumulation: the standardised
+// inputs and the first layer's activations are rounded to BF16 where they enter a
+// tensor-core product (the weights already are BF16).  The accumulator fragments of
+// two neighbouring 8-column tiles of one layer hold exactly the A fragment of the
+// next layer's 16-column step, so activations never leave registers.  Layer 3
+// (64 -> 2) is a dot product per sample over the warp's fragments, reduced across
+// the four lanes that share a row.
+
+__device__ __forceinline__ uint32_t packBf16(float lo, float hi)
+{
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);     // .x = lo (low half)
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+__device__ __forceinline__ void mmaBf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
+{
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+                 "{%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+constexpr int kTensorWarps = 4;                     // 64 samples per CTA
+
+__global__ void __launch_bounds__(kTensorWarps * 32) forwardTensorKernel(const float* __restrict__ params,
+                                                                         const float* __restrict__ norm,
+                                                                         const float* __restrict__ x, int n,
+                                                                         float* __restrict__ y)
+{
+    __shared__ Staged s;
+    stage(s, params, norm);
+    __syncthreads();
+    const int lane = int(threadIdx.x & 31), warp = int(threadIdx.x >> 5);
+    const int group = lane >> 2, quad = lane & 3;   // fragment row group and column pair
+    const int rowBase = (blockIdx.x * kTensorWarps + warp) * 16;
+    const int rows[2] = {rowBase + group, rowBase + group + 8};
+    // Layer-1 A fragment: inputs (rows g, g+8; columns 2q, 2q+1, 2q+8, 2q+9).
+    float in[2][4];
+    for (int r = 0; r < 2; ++r) {
+        const bool live = rows[r] < n;
+        const float* row = x + size_t(live ? rows[r] : 0) * F;
+        const int cols[4] = {2 * quad, 2 * quad + 1, 2 * quad + 8, 2 * quad + 9};
+        for (int c = 0; c < 4; ++c)
+            in[r][c] = live ? (row[cols[c]] - s.mean[cols[c]]) * s.invStd[cols[c]] : 0.f;
+    }
+    const uint32_t a1[4] = {packBf16(in[0][0], in[0][1]), packBf16(in[1][0], in[1][1]),
+                            packBf16(in[0][2], in[0][3]), packBf16(in[1][2], in[1][3])};
+    // Layer 1: 8 column tiles of 8 outputs.
+    float h1[8][4];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        const int out = 8 * t + group;              // B column = output index
+        const uint32_t b0 = packBf16(s.w1[out * F + 2 * quad], s.w1[out * F + 2 * quad + 1]);
+        const uint32_t b1 = packBf16(s.w1[out * F + 2 * quad + 8], s.w1[out * F + 2 * quad + 9]);
+        const float bias0 = s.b1[8 * t + 2 * quad], bias1 = s.b1[8 * t + 2 * quad + 1];
+        h1[t][0] = bias0;
+        h1[t][1] = bias1;
+        h1[t][2] = bias0;
+        h1[t][3] = bias1;
+        mmaBf16(h1[t], a1, b0, b1);
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            h1[t][c] = fmaxf(h1[t][c], 0.f);
+    }
+    // Layer 2: 4 steps of 16 inputs (two layer-1 tiles each) x 8 output tiles.
+    float h2[8][4];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        const float bias0 = s.b2[8 * t + 2 * quad], bias1 = s.b2[8 * t + 2 * quad + 1];
+        h2[t][0] = bias0;
+        h2[t][1] = bias1;
+        h2[t][2] = bias0;
+        h2[t][3] = bias1;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t a[4] = {packBf16(h1[2 * k][0], h1[2 * k][1]), packBf16(h1[2 * k][2], h1[2 * k][3]),
+                               packBf16(h1[2 * k + 1][0], h1[2 * k + 1][1]),
+                               packBf16(h1[2 * k + 1][2], h1[2 * k + 1][3])};
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            const int out = 8 * t + group;
+            const float* w = s.w2 + out * H + 16 * k;
+            mmaBf16(h2[t], a, packBf16(w[2 * quad], w[2 * quad + 1]), packBf16(w[2 * quad + 8], w[2 * quad + 9]));
+        }
+    }
+    // Layer 3: the lane's partial sums for rows g and g+8, then across the quad.
+    float part[2][O] = {{0.f, 0.f}, {0.f, 0.f}};
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int j = 8 * t + 2 * quad + (c & 1);
+            const float a = fmaxf(h2[t][c], 0.f);
+            part[c >> 1][0] = fmaf(s.w3[j], a, part[c >> 1][0]);
+            part[c >> 1][1] = fmaf(s.w3[H + j], a, part[c >> 1][1]);
+        }
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int o = 0; o < O; ++o) {
+            part[r][o] += __shfl_xor_sync(0xffffffffu, part[r][o], 1);
+            part[r][o] += __shfl_xor_sync(0xffffffffu, part[r][o], 2);
+        }
+    if (quad == 0)
+        for (int r = 0; r < 2; ++r)
+            if (rows[r] < n)
+                for (int o = 0; o < O; ++o)
+                    y[2 * size_t(rows[r]) + o] = fmaf(part[r][o] + s.b3[o], s.targetStd[o], s.targetMean[o]);
+}
+
 constexpr size_t kGradientSmem =
     sizeof(Staged) + sizeof(float) * (size_t(kSamples) * (kXStride + 4 * kHStride + O) + kSamples);
 
@@ -368,8 +482,9 @@ int cs_lifetime_forward(const float* params, const float* norm, const float* fea
         requireAligned(norm, "norm");
         requireAligned(features, "features");
         requireAligned(predictions, "predictions");
-        forwardKernel<<<blocksFor(count), kSamples, 0, cudaStream_t(stream)>>>(params, norm, features, count,
-                                                                                predictions);
+        const int warpsRows = kTensorWarps * 16;
+        forwardTensorKernel<<<(count + warpsRows - 1) / warpsRows, kTensorWarps * 32, 0, cudaStream_t(stream)>>>(
+            params, norm, features, count, predictions);
         check(cudaGetLastError(), "forward kernel launch");
     });
 }

@@ -15,6 +15,7 @@
 #include <chrono>
 #include <climits>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <deque>
@@ -263,6 +264,7 @@ struct SegmentTables {
     std::vector<int4> tileRuns;         // (span, first frame, end frame, first tile) per span
     size_t tileCount = 0;               // source tiles of all segments
     size_t scratchBytes = 0;
+    size_t fullScratchBytes = 0;        // chain storage of the whole timeline in one segment
 };
 
 // A chain runs on the one-recurrence-per-lane kernel when every span filters
@@ -382,6 +384,14 @@ SegmentTables planSegments(const HostBatch& batch, size_t budget)
         phasesPerBlock[size_t(b)] += phasesRun;
     }
 
+    {
+        size_t floats = 0, phases = 0;
+        for (int b = 0; b < blocks; ++b) {
+            floats += size_t(floatsPerBlock[size_t(b)]);
+            phases += size_t(phasesPerBlock[size_t(b)]);
+        }
+        t.fullScratchBytes = scratchBytesOf(floats, phases);
+    }
     std::vector<std::pair<int, int>> ranges;
     for (int b = 0; b < blocks;) {
         size_t floats = 0, phases = 0;
@@ -765,6 +775,9 @@ struct cs_renderer {
     bool sharedSources = true;          // render each shared voice source once per batch
     size_t budgetCache = 0;             // derived scratch budget of the current render call (0: stale)
     size_t deferred = 0;                // serving: launches deferred for lack of free memory
+    struct FailedRequest {              // sizes of the last batch whose arena did not fit
+        size_t requested = 0, mix = 0, scratch = 0, finishing = 0, metadata = 0;
+    } failed;
     std::string error;                  // message of this renderer's last failed call
     // Host time spent staging batches, per phase (cs_renderer_host_ms).
     double hostMs[cs::kHostPhases] = {};
@@ -849,7 +862,8 @@ bool pageLocked(const void* pointer)
 
 // `shared`: carve the batch from the renderer's reusable arena (render_window
 // batches, one alive at a time) instead of a dedicated allocation.
-cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool shared = false, int laneIndex = 0)
+cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool shared = false, int laneIndex = 0,
+                     size_t firstJob = 0)
 {
     check(cudaSetDevice(r.device), "CUDA device");
     auto p = std::make_unique<cs_prepared>();
@@ -883,6 +897,9 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     r.hostMs[1] += msSince(mark);
     p->tables = planSegments(batch, scratchBudget);
     const SegmentTables& t = p->tables;
+    if (t.segments.size() > 1)          // the reference's protocol line for segmented synthesis
+        std::fprintf(stderr, "SEGMENT\tfirst=%zu\tjobs=%zu\tcount=%zu\tscratch_bytes=%zu\tfull_scratch_bytes=%zu\n",
+                     firstJob, count, t.segments.size(), t.scratchBytes, t.fullScratchBytes);
     r.hostMs[2] += msSince(mark);
     if (r.sharedSources)
         p->shared = planSharedSources(batch, scratchBudget / 2);
@@ -951,6 +968,8 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
             if (status != cudaSuccess) {
                 cudaGetLastError();
                 lane.arena = nullptr;
+                r.failed = {p->arenaBytes, p->mixBytes, t.scratchBytes, oScratch - oMix - p->mixBytes,
+                            uploadEnd};
                 throw CudaError(status, "CUDA batch arena allocation");
             }
             lane.arenaCapacity = p->arenaBytes;
@@ -1372,6 +1391,8 @@ public:
                 break;
             publishFront();
         }
+        // The reference's summary line of a render window (jobs, batches, refills).
+        std::fprintf(stderr, "SCHEDULE\tjobs=%zu\trounds=%zu\trefills=%zu\n", queue.size(), rounds, refills);
     }
 
     // cs_submit: queues plans and launches what the free lanes take; returns the
@@ -1455,6 +1476,7 @@ public:
 private:
     size_t next = 0;                            // first queued plan not yet launched
     size_t ticketBase = 0;                      // tickets of the plans dropped from the queue
+    size_t rounds = 0, refills = 0;             // batches launched, refills taken
 
     // Keeps up to laneCount batches in flight: the next batch is staged and
     // launched on a free lane while the others run.  `mayRefill`: ask the refill
@@ -1502,6 +1524,7 @@ private:
             }
             run(r, *prepared, nullptr);
             enqueueDownload(r, *prepared);
+            ++rounds;
             flight.push_back({prepared, next});
             next += jobs;
             freeKnown = false;
@@ -1550,6 +1573,7 @@ private:
             return false;
         checkPlans(plans, count);
         queue.insert(queue.end(), plans, plans + count);
+        ++refills;
         return true;
     }
 
@@ -1581,7 +1605,7 @@ private:
     {
         for (;;) {
             try {
-                return prepare(r, queue.data() + first, jobs, true, lane);
+                return prepare(r, queue.data() + first, jobs, true, lane, ticketBase + first);
             } catch (const CudaError& e) {
                 if (e.code != cudaErrorMemoryAllocation)
                     throw;
@@ -1608,6 +1632,13 @@ private:
                     jobs = batchEnd(first, first + jobs / 2) - first;
                     continue;
                 }
+                size_t freeBytes = 0, total = 0;
+                cudaMemGetInfo(&freeBytes, &total);
+                std::fprintf(stderr, "MEMORY\tjob=%zu\trequested_bytes=%zu\tmix_bytes=%zu\tfilter_bytes=%zu"
+                                     "\tfinishing_bytes=%zu\tmetadata_bytes=%zu\tsample_bytes=%zu"
+                                     "\tfree_device_bytes=%zu\n",
+                             ticketBase + first, r.failed.requested, r.failed.mix, r.failed.scratch,
+                             r.failed.finishing, r.failed.metadata, r.uploaded * sizeof(float), freeBytes);
                 return nullptr;
             }
         }

@@ -50,11 +50,20 @@ def _standardise(norm: np.ndarray, features: np.ndarray) -> np.ndarray:
     return (np.asarray(features, np.float64) - norm[:F]) * norm[F:2 * F]
 
 
-def forward(params: np.ndarray, norm: np.ndarray, features: np.ndarray, rounding: bool = True) -> np.ndarray:
-    """Predictions in target units, shape (n, 2)."""
+def forward(params: np.ndarray, norm: np.ndarray, features: np.ndarray, rounding: bool = True,
+            tensor: bool = True) -> np.ndarray:
+    """Predictions in target units, shape (n, 2).  `tensor`: the inference kernel's
+    numerics, whose first two layers run on BF16 tensor cores, so the standardised
+    inputs and the first layer's activations are rounded to BF16 where they enter
+    those products (cs_lifetime_forward); the training kernels keep them in FP32."""
     w1, b1, w2, b2, w3, b3 = unpack(params, rounding)
     norm = np.asarray(norm, np.float64)
-    h1 = np.maximum(_standardise(norm, features) @ w1.T + b1, 0)
+    x = _standardise(norm, features)
+    if tensor:
+        x = bf16(x.astype(np.float32))
+    h1 = np.maximum(x @ w1.T + b1, 0)
+    if tensor:
+        h1 = bf16(h1.astype(np.float32))
     h2 = np.maximum(h1 @ w2.T + b2, 0)
     y = h2 @ w3.T + b3
     return y * norm[2 * F + O:] + norm[2 * F:2 * F + O]
@@ -89,7 +98,8 @@ def gradient(params: np.ndarray, norm: np.ndarray, features: np.ndarray, targets
 
 
 def loss(params, norm, features, targets, rounding: bool = True) -> float:
-    y = forward(params, norm, features, rounding)
+    """The training loss (FP32 activations, as the training kernels compute them)."""
+    y = forward(params, norm, features, rounding, tensor=False)
     norm = np.asarray(norm, np.float64)
     std = norm[2 * F + O:]
     err = (y - np.asarray(targets, np.float64)) / std
