@@ -379,6 +379,27 @@ def cpu_baseline(jobs, sample_jobs, host_plans, host_bank, renderer):
     return baseline, parity
 
 
+def reference_gpu(jobs, stage_ms, audio):
+    """The reference's own synthesis kernels (its render.cu built for this GPU with
+    the NVRTC defaults, launched as its renderer launches them for one segment) on
+    every job of the workload, planned by the reference planner: device time of the
+    synthesis launches against this package's synthesis stages on the same jobs
+    (finishing excluded on both sides)."""
+    from oracle import reference
+    if not reference.gpu_available():
+        raise RuntimeError("oracle/_ref/libclayref_gpu.so is not built")
+    session = reference.RefSession()
+    plans = [session.plan(sfz, midi, tail="natural") for sfz, midi in jobs]
+    bank = session.bank()
+    session.close()
+    ms = reference.time_gpu(plans, bank, repeats=3)
+    ours = sum(v for k, v in stage_ms.items() if k not in ("finish", "assess"))
+    return {"synthesis_ms": ms, "ours_synthesis_ms": ours, "speedup": ms / ours if ours else None,
+            "reference_audio_s_per_s": audio / (ms * 1e-3), "jobs": len(plans),
+            "what": "src/cuda/render.cu kernels (pitch, filter sources, filters, tiles) on this GPU, "
+                    "device time, one segment; ours: the shared-source, source, recurrence and mix stages"}
+
+
 def run_reference(args):
     rank, world, _ = dist_info()
     if rank != 0:
@@ -583,6 +604,10 @@ def run_b200(args):
                 out["cpu_baseline"], out["parity"] = cpu_baseline(jobs, sample_jobs(args), plans, bank, renderer)
             except Exception as error:
                 out["cpu_baseline"] = {"value": None, "unavailable": str(error)}
+            try:
+                out["reference_gpu"] = reference_gpu(jobs, stage_ms, audio)
+            except Exception as error:
+                out["reference_gpu"] = {"unavailable": str(error)}
         print(json.dumps(out))
     prepared.close()
     renderer.close()

@@ -69,7 +69,19 @@ const char* ref_gpu_last_error(void) { return lastError.c_str(); }
 // Float mix (float2 per frame, jobs concatenated in plan order) of `count` plans
 // rendered by the reference's kernels on the current device.  `mix` is host
 // memory of sum(frames) float2.  Returns 0 on success.
+int ref_gpu_synthesize_timed(const cs_plan* plans, int count, const float* bank, size_t bankFloats, void* mix,
+                             int repeats, float* ms);
+
 int ref_gpu_synthesize(const cs_plan* plans, int count, const float* bank, size_t bankFloats, void* mix)
+{
+    return ref_gpu_synthesize_timed(plans, count, bank, bankFloats, mix, 0, nullptr);
+}
+
+// As ref_gpu_synthesize; with `repeats` > 0 the launch sequence then runs that
+// many more times on the device-resident batch and `ms` receives the mean device
+// time of one sequence (CUDA events around the launches).
+int ref_gpu_synthesize_timed(const cs_plan* plans, int count, const float* bank, size_t bankFloats, void* mix,
+                             int repeats, float* ms)
 {
     try {
         HostBatch batch;
@@ -102,23 +114,47 @@ int ref_gpu_synthesize(const cs_plan* plans, int count, const float* bank, size_
         // tileFrames threads (every kernel bounds-checks its index).
         constexpr int chainThreads = 32;
         const int pitchCount = int(batch.pitchHeads.size());
-        if (pitchCount)
-            prepareVoicePitch<<<(pitchCount + chainThreads - 1) / chainThreads, chainThreads>>>(
-                dVoices, dPitchHeads, dControls, dModulation, dPhase, dStates, first, end, frames, pitchCount);
         const int sourceCount = int(batch.filterTiles.size());
-        if (sourceCount)
-            renderFilterSources<<<sourceCount, tileFrames>>>(dSamples, dSinc, dVoices, dFilterTiles, dControls,
-                                                             dModulation, dPhase, dFiltered, first, end, frames, 0);
         const int filterCount = int(batch.filterHeads.size());
-        if (filterCount)
-            applyVoiceFilters<<<(filterCount + chainThreads - 1) / chainThreads, chainThreads>>>(
-                dVoices, dFilterHeads, dControls, dModulation, dFiltered, dStates, first, end, frames, filterCount);
         const int tileCount = int(batch.tiles.size());
-        if (tileCount)
-            renderTiles<<<tileCount, tileFrames>>>(dSamples, dSinc, dVoices, dTiles, dIndices, dControls, dModulation,
-                                                   dFiltered, dOutput, first, end, frames, 0);
+        const auto sequence = [&] {
+            if (pitchCount)
+                prepareVoicePitch<<<(pitchCount + chainThreads - 1) / chainThreads, chainThreads>>>(
+                    dVoices, dPitchHeads, dControls, dModulation, dPhase, dStates, first, end, frames, pitchCount);
+            if (sourceCount)
+                renderFilterSources<<<sourceCount, tileFrames>>>(dSamples, dSinc, dVoices, dFilterTiles, dControls,
+                                                                 dModulation, dPhase, dFiltered, first, end, frames, 0);
+            if (filterCount)
+                applyVoiceFilters<<<(filterCount + chainThreads - 1) / chainThreads, chainThreads>>>(
+                    dVoices, dFilterHeads, dControls, dModulation, dFiltered, dStates, first, end, frames, filterCount);
+            if (tileCount)
+                renderTiles<<<tileCount, tileFrames>>>(dSamples, dSinc, dVoices, dTiles, dIndices, dControls,
+                                                       dModulation, dFiltered, dOutput, first, end, frames, 0);
+        };
+        sequence();
         DeviceBuffers::check(cudaGetLastError(), "launch");
         DeviceBuffers::check(cudaDeviceSynchronize(), "render");
+        if (repeats > 0 && ms) {
+            // Chain state restarts from zero for every run of the sequence.
+            const size_t stateBytes = std::max<size_t>(batch.voices.size() * sizeof(VoiceState), 16);
+            cudaEvent_t start, stop;
+            DeviceBuffers::check(cudaEventCreate(&start), "event");
+            DeviceBuffers::check(cudaEventCreate(&stop), "event");
+            float total = 0;
+            for (int k = 0; k < repeats; ++k) {
+                DeviceBuffers::check(cudaMemset(dStates, 0, stateBytes), "clear");
+                DeviceBuffers::check(cudaEventRecord(start), "event");
+                sequence();
+                DeviceBuffers::check(cudaEventRecord(stop), "event");
+                DeviceBuffers::check(cudaEventSynchronize(stop), "render");
+                float once = 0;
+                DeviceBuffers::check(cudaEventElapsedTime(&once, start, stop), "timing");
+                total += once;
+            }
+            cudaEventDestroy(start);
+            cudaEventDestroy(stop);
+            *ms = total / float(repeats);
+        }
         DeviceBuffers::check(cudaMemcpy(mix, dOutput, batch.frames * sizeof(float2), cudaMemcpyDeviceToHost),
                              "download");
         return 0;

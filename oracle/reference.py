@@ -56,6 +56,8 @@ def gpu_lib():
         _gpu.ref_gpu_last_error.restype = ctypes.c_char_p
         _gpu.ref_gpu_synthesize.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t,
                                             ctypes.c_void_p]
+        _gpu.ref_gpu_synthesize_timed.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t,
+                                                  ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
     return _gpu
 
 
@@ -70,6 +72,20 @@ def synthesize_gpu(plans: list[Plan], bank: np.ndarray) -> np.ndarray:
                                     out.ctypes.data):
         raise RuntimeError(gpu_lib().ref_gpu_last_error().decode())
     return out
+
+
+def time_gpu(plans: list[Plan], bank: np.ndarray, repeats: int = 5) -> float:
+    """Mean device milliseconds of the reference's synthesis launches (render.cu on
+    this GPU, one segment) over `repeats` runs after a first one."""
+    frames = sum(p.frames for p in plans)
+    out = np.zeros((frames, 2), np.float32)
+    array = c_plans(plans)
+    bank = np.ascontiguousarray(bank, np.float32)
+    ms = ctypes.c_float()
+    if gpu_lib().ref_gpu_synthesize_timed(array, len(plans), bank.ctypes.data if bank.size else None, bank.size,
+                                          out.ctypes.data, repeats, ctypes.byref(ms)):
+        raise RuntimeError(gpu_lib().ref_gpu_last_error().decode())
+    return float(ms.value)
 
 
 def lib():
