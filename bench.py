@@ -61,10 +61,12 @@ WORKLOADS = {
     "plain_batch": WORKLOAD,
     "uneven": "uneven batch: 1024 jobs over 4 presets of 12 mono 16-bit regions (48-tap sinc resampling, "
               "no filter), Pareto(1.5) lengths 2-600 s",
+    "uneven_hbm": "uneven batch with an HBM-resident bank: 1024 jobs over 4 presets of 22 keycenters x 8 "
+                  "velocity layers x 48 s mono (about 6 GB of float samples), Pareto(1.5) lengths 2-600 s",
 }
 # Jobs of the bounded CPU sample (the reference arm's step and the cpu_baseline /
 # parity leg): about 1-6 s of the reference's host render on 16 cores.
-CPU_SAMPLE_JOBS = {"plain_batch": 16, "uneven": 128}
+CPU_SAMPLE_JOBS = {"plain_batch": 16, "uneven": 128, "uneven_hbm": 64}
 
 
 def parse():
@@ -117,12 +119,14 @@ def workload(args, rank):
     from claysampler_b200 import workload as wl
     kind = getattr(args, "workload", "plain_batch")
     if args.jobs is None:
-        args.jobs = 1024 if kind == "uneven" else 64
+        args.jobs = 1024 if kind.startswith("uneven") else 64
     root = args.workdir / f"{kind}_s{args.seed + rank}_j{args.jobs}"
     marker = root / "ready"
     if not marker.exists():
         if kind == "uneven":
             jobs = wl.write_uneven_batch(root, seed=args.seed + rank, jobs=args.jobs)
+        elif kind == "uneven_hbm":
+            jobs = wl.write_uneven_hbm_batch(root, seed=args.seed + rank, jobs=args.jobs)
         else:
             jobs = wl.write_plain_batch(root, seed=args.seed + rank, jobs=args.jobs)
         marker.write_text("\n".join(f"{j.sfz}\t{j.midi}" for j in jobs))

@@ -775,6 +775,8 @@ struct cs_renderer {
     bool sharedSources = true;          // render each shared voice source once per batch
     size_t budgetCache = 0;             // derived scratch budget of the current render call (0: stale)
     size_t deferred = 0;                // serving: launches deferred for lack of free memory
+    size_t oomBudget = 0;               // scratch cap after a lone job's arena did not fit (0: none)
+    int failAllocations = 0;            // host-side fault injection: batch arenas to refuse
     struct FailedRequest {              // sizes of the last batch whose arena did not fit
         size_t requested = 0, mix = 0, scratch = 0, finishing = 0, metadata = 0;
     } failed;
@@ -893,7 +895,9 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     // The derived budget is read once per render call (cudaMemGetInfo is slow).
     if (!r.scratchLimit && !r.budgetCache)
         r.budgetCache = defaultScratchBudget();
-    const size_t scratchBudget = r.scratchLimit ? r.scratchLimit : r.budgetCache;
+    size_t scratchBudget = r.scratchLimit ? r.scratchLimit : r.budgetCache;
+    if (r.oomBudget)
+        scratchBudget = std::min(scratchBudget, r.oomBudget);
     r.hostMs[1] += msSince(mark);
     p->tables = planSegments(batch, scratchBudget);
     const SegmentTables& t = p->tables;
@@ -964,7 +968,10 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
             r.live -= lane.arenaCapacity;
             lane.arena = nullptr;
             lane.arenaCapacity = 0;
-            cudaError_t status = cudaMalloc(&lane.arena, p->arenaBytes);
+            cudaError_t status = r.failAllocations > 0 ? cudaErrorMemoryAllocation
+                                                       : cudaMalloc(&lane.arena, p->arenaBytes);
+            if (r.failAllocations > 0)
+                --r.failAllocations;
             if (status != cudaSuccess) {
                 cudaGetLastError();
                 lane.arena = nullptr;
@@ -978,10 +985,13 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
         p->arena = lane.arena;
         p->sharedArena = true;
     } else {
-        cudaError_t status = cudaMalloc(&p->arena, p->arenaBytes);
+        cudaError_t status = r.failAllocations > 0 ? cudaErrorMemoryAllocation : cudaMalloc(&p->arena, p->arenaBytes);
+        if (r.failAllocations > 0)
+            --r.failAllocations;
         if (status != cudaSuccess) {
             cudaGetLastError();
             p->arena = nullptr;
+            r.failed = {p->arenaBytes, p->mixBytes, t.scratchBytes, oScratch - oMix - p->mixBytes, uploadEnd};
             throw CudaError(status, "CUDA batch arena allocation");
         }
         r.live += p->arenaBytes;
@@ -1383,6 +1393,7 @@ public:
     void render(const cs_plan* plans, size_t count)
     {
         r.budgetCache = 0;
+        r.oomBudget = 0;
         queue.assign(plans, plans + count);
         next = 0;
         for (;;) {
@@ -1401,6 +1412,7 @@ public:
     {
         const size_t ticket = ticketBase + queue.size();
         r.budgetCache = 0;
+        r.oomBudget = 0;
         queue.insert(queue.end(), plans, plans + count);
         launch(false, true);
         return ticket;
@@ -1632,6 +1644,15 @@ private:
                     jobs = batchEnd(first, first + jobs / 2) - first;
                     continue;
                 }
+                // A lone job whose chain scratch dominates: halve the scratch budget,
+                // so the job renders in more segments (src/cuda/renderer.cpp:950-953).
+                // (The budget only ever shrinks, so the ladder ends.)
+                const size_t halved = r.failed.scratch / 2;
+                if (r.failed.scratch > std::max<size_t>(r.failed.finishing, size_t(2) << 20) &&
+                    (!r.oomBudget || halved < r.oomBudget)) {
+                    r.oomBudget = halved;
+                    continue;
+                }
                 size_t freeBytes = 0, total = 0;
                 cudaMemGetInfo(&freeBytes, &total);
                 std::fprintf(stderr, "MEMORY\tjob=%zu\trequested_bytes=%zu\tmix_bytes=%zu\tfilter_bytes=%zu"
@@ -1733,7 +1754,7 @@ private:
     void rejectScratch(size_t first)
     {
         cs_batch rejected{};
-        rejected.failed_scratch_bytes = 1;
+        rejected.failed_scratch_bytes = std::max<size_t>(r.failed.requested, 1);
         publish(user, &rejected, ticketBase + first);
     }
 
@@ -2263,6 +2284,15 @@ int cs_renderer_set_scratch_limit(cs_renderer* r, size_t bytes)
         if (!r)
             throw std::runtime_error("null renderer");
         r->scratchLimit = bytes;
+    });
+}
+
+int cs_renderer_fail_allocations(cs_renderer* r, int count)
+{
+    return cs::guardedOn(r, [&] {
+        if (!r || count < 0)
+            throw std::runtime_error("invalid allocation-failure count");
+        r->failAllocations = count;
     });
 }
 

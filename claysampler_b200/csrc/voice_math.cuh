@@ -1,8 +1,9 @@
 // Per-voice, per-frame arithmetic of the render path.  Each function restates the
 // reference's definition (src/cuda/render.cu) operation for operation, because the
 // float bus is checked against the reference within 1e-5 of full scale and PCM16 to
-// one LSB: the build uses --fmad=false so only the explicit fmaf calls fuse, as in
-// the reference compiled for the host.
+// one LSB.  The build contracts multiply-adds as the reference's NVRTC build does
+// (nvcc's default), and with the same expressions the compiler fuses the same
+// pairs: the mix comes out bit-identical to the reference's own kernels on the GPU.
 #pragma once
 
 #include "kernels.cuh"

@@ -313,3 +313,57 @@ def write_serving_jobs(root: Path, seed: int = 5, jobs: int = 200, presets: int 
         _note_midi(notes, [], float(seconds), midi)
         out.append(Job("-", sfzs[j % presets], midi, root / "out" / f"serve_{j:04d}.wav"))
     return out, arrivals
+
+
+def write_hbm_preset(root: Path, seed: int, name: str, centers: range = range(23, 109, 4), layers: int = 8,
+                     seconds: float = 48.0) -> Path:
+    """A large mono 16-bit multisample: a region per keycenter (every 4 semitones,
+    keys -2..+1 around it) and velocity layer, each `seconds` long.  Each sample
+    tiles one period of an 8-partial wavetable (brighter for louder layers) under an
+    exponential decay, which keeps generating gigabytes of samples fast."""
+    rng = np.random.default_rng(seed)
+    samples = root / f"{name}_samples"
+    samples.mkdir(parents=True, exist_ok=True)
+    frames = int(seconds * RATE)
+    edges = np.linspace(0, 128, layers + 1).astype(int)
+    lines = ["<group> ampeg_attack=0.005 ampeg_decay=0.2 ampeg_sustain=60 ampeg_release=0.3 loop_mode=no_loop\n"]
+    t = np.arange(frames) / RATE
+    for center in centers:
+        period = max(2, int(round(RATE / key_frequency(center))))
+        phase = np.arange(period) / period
+        decay = np.exp(-t / float(rng.uniform(4.0, 12.0)))
+        for layer in range(layers):
+            bright = 0.3 + 0.7 * layer / max(1, layers - 1)
+            table = np.zeros(period)
+            for k in range(1, 9):
+                table += (bright ** (k - 1)) * float(rng.uniform(0.6, 1.0)) / k * \
+                    np.sin(2 * np.pi * k * phase + float(rng.uniform(0, 2 * np.pi)))
+            table *= 0.45 / max(1e-9, float(np.max(np.abs(table))))
+            data = np.resize(table, frames) * decay
+            wav = samples / f"c{center:03d}_v{layer}.wav"
+            write_wav(wav, data, bits=16)
+            lo, hi = max(21, center - 2), min(108, center + 1)
+            lines.append(f"<region> sample={wav.relative_to(root).as_posix()} lokey={lo} hikey={hi} "
+                         f"pitch_keycenter={center} lovel={max(1, int(edges[layer]))} hivel={int(edges[layer + 1]) - 1}\n")
+    sfz = root / f"{name}.sfz"
+    sfz.write_text("".join(lines), encoding="ascii")
+    return sfz
+
+
+def write_uneven_hbm_batch(root: Path, seed: int = 3, jobs: int = 1024, presets: int = 4,
+                           high: float = 600.0) -> list[Job]:
+    """The uneven batch over four large presets (about 6 GB of float samples in
+    all, far above the L2): Pareto(1.5) lengths from 2 to 600 s, notes as in the
+    small kind with velocities spanning the layers."""
+    root.mkdir(parents=True, exist_ok=True)
+    sfzs = [write_hbm_preset(root, seed + p, name=f"large{p}") for p in range(presets)]
+    rng = np.random.default_rng(seed + 1000)
+    lengths = pareto_seconds(rng, jobs, high=high)
+    out = []
+    for j, seconds in enumerate(lengths):
+        count = max(1, int(round(64 * seconds / 30.0)))
+        notes = _performance(rng, float(seconds), None, count, 1, 127, 0.5)
+        midi = root / f"uneven_hbm_{j:04d}.mid"
+        _note_midi(notes, [], float(seconds), midi)
+        out.append(Job("-", sfzs[j % presets], midi, root / "out" / f"uneven_hbm_{j:04d}.wav"))
+    return out

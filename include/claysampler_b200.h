@@ -282,6 +282,12 @@ int cs_renderer_host_ms(const cs_renderer* renderer, double* ms, int capacity);
  * as they finish.  The reference keeps one rolling batch of resident jobs
  * (src/cuda/renderer.cpp:1353-1746). */
 int cs_renderer_set_lanes(cs_renderer* renderer, int lanes);
+/* Host-side fault injection for tests: the next `count` batch-arena allocations
+ * report cudaErrorMemoryAllocation without calling the allocator, so the
+ * out-of-memory ladder of cs_render_window / cs_poll runs (publish the batches in
+ * flight and free the other lanes' arenas, halve the batch, halve a lone job's
+ * scratch budget, reject the job; src/cuda/renderer.cpp:947-992).  0 turns it off. */
+int cs_renderer_fail_allocations(cs_renderer* renderer, int count);
 /* Serving: how often a batch launch waited because its estimated footprint
  * exceeded half of the free device memory while other batches were in flight. */
 size_t cs_renderer_deferred_launches(const cs_renderer* renderer);

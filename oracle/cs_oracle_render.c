@@ -42,6 +42,7 @@ typedef struct {                /* Tile, render_types.h:70-74 */
 typedef struct {
     const float* bank;
     const float* sinc;          /* tap-major [48][2049], as the reference */
+    const double* sinc64;       /* the same table before its FP32 rounding (FP64 resampler mode) */
     cs_voice_span* voices;
     int voiceCount;
     cs_control_point* points;
@@ -63,8 +64,9 @@ typedef struct {
 
 static F2 f2(float x, float y) { F2 v = {x, y}; return v; }
 
-/* renderer.cpp:347-376 */
-static void sincTable(float* table)
+/* renderer.cpp:347-376; `wide` receives the FP64 values before the FP32
+ * rounding the reference applies (renderer.cpp:370-371), when not null. */
+static void sincTableBoth(float* table, double* wide)
 {
     const double beta = 8.5, pi = 3.14159265358979323846;
     double norm;
@@ -89,10 +91,14 @@ static void sincTable(float* table)
                 if (term < 1e-14) break;
             }
             const double window = sum / norm;
-            table[tap * (PHASES + 1) + phase] = (float)(window * (x == 0 ? 1 : sin(pi * x) / (pi * x)));
+            const double value64 = window * (x == 0 ? 1 : sin(pi * x) / (pi * x));
+            if (table) table[tap * (PHASES + 1) + phase] = (float)value64;
+            if (wide) wide[tap * (PHASES + 1) + phase] = value64;
         }
     }
 }
+
+static void sincTable(float* table) { sincTableBoth(table, NULL); }
 
 /* render.cu:6-19 (amplitude, filter and pitch envelopes share the fields) */
 static float envelopeSpan(const cs_voice_span* e, int frame)
@@ -130,9 +136,29 @@ static F2 fetch(const float* bank, const cs_voice_span* v, int frame)
     return f2(left, v->channels == 1 ? left : bank[index + 1]);
 }
 
-/* render.cu:30-61 */
-static F2 interpolateAt(const float* bank, const float* sinc, const cs_voice_span* v, double pos)
+/* render.cu:30-61 in FP64: the unrounded table, products and sums in double,
+ * rounded to float once at the end.  Bounds the FP32 resampler's error
+ * independently of the reference's own FP32 arithmetic. */
+static F2 interpolateAt64(const float* bank, const double* sinc, const cs_voice_span* v, double pos)
 {
+    const int center = (int)floor(pos);
+    if (pos == center) return fetch(bank, v, center);
+    const int phase = (int)nearbyint((pos - center) * PHASES);
+    double x = 0, y = 0;
+    for (int tap = 0; tap < TAPS; ++tap) {
+        const F2 s = fetch(bank, v, center - 23 + tap);
+        const double w = sinc[tap * (PHASES + 1) + phase];
+        x += w * (double)s.x;
+        y += w * (double)s.y;
+    }
+    return f2((float)x, (float)y);
+}
+
+/* render.cu:30-61 */
+static F2 interpolateAt(const float* bank, const float* sinc, const double* sinc64, const cs_voice_span* v,
+                        double pos)
+{
+    if (sinc64) return interpolateAt64(bank, sinc64, v, pos);
     const int center = (int)floor(pos);
     if (pos == center) return fetch(bank, v, center);
     const int phase = (int)nearbyint((pos - center) * PHASES);
@@ -162,7 +188,8 @@ static F2 interpolateAt(const float* bank, const float* sinc, const cs_voice_spa
 }
 
 /* render.cu:63-100 */
-static F2 interpolate(const float* bank, const float* sinc, const cs_voice_span* v, int frame, double pos)
+static F2 interpolate(const float* bank, const float* sinc, const double* sinc64, const cs_voice_span* v, int frame,
+                      double pos)
 {
     if (pos < 0) {
         const int elapsed = frame - v->begin;
@@ -185,10 +212,10 @@ static F2 interpolate(const float* bank, const float* sinc, const cs_voice_span*
     const int period = v->loopEnd - v->loopFirst;
     if (v->loopEnd > 0 && pos >= v->loopEnd) pos = v->loopFirst + fmod(pos - v->loopFirst, (double)period);
     if (pos >= v->sourceEnd) return f2(0, 0);
-    F2 sample = interpolateAt(bank, sinc, v, pos);
+    F2 sample = interpolateAt(bank, sinc, sinc64, v, pos);
     const int fadeStart = v->loopEnd - v->loopCrossfade;
     if (v->loopEnd > 0 && v->loopCrossfade > 0 && pos >= fadeStart) {
-        const F2 entry = interpolateAt(bank, sinc, v, pos - period);
+        const F2 entry = interpolateAt(bank, sinc, sinc64, v, pos - period);
         const float phase = (float)((pos - fadeStart) / v->loopCrossfade);
         const float blend = .5f - .5f * cosf(3.14159265358979323846f * phase);
         sample.x = fmaf(blend, entry.x - sample.x, sample.x);
@@ -248,7 +275,7 @@ static F2 voiceAudio(const Batch* b, const cs_voice_span* v, float pan, int fram
         }
     }
     if (db != 0) level *= exp2f(db * .166096404744368f);
-    const F2 sample = interpolate(b->bank, b->sinc, v, frame, phase);
+    const F2 sample = interpolate(b->bank, b->sinc, b->sinc64, v, frame, phase);
     if (filterInput && v->channels == 1) return f2(sample.x * level, sample.x * level);
     const F2 gains = panGains(v, pan);
     const float l = sample.x * gains.x, r = sample.y * gains.y;
@@ -644,16 +671,18 @@ static void freeBatch(Batch* b)
     free(b->states);
 }
 
-/* The batch's mix: float2 per frame (natural) or short2 (orig/custom), jobs
- * concatenated in plan order. */
-int oracle_synthesize(const cs_plan* plans, int count, const float* bank, int natural, int threads, void* out)
+static int synthesize(const cs_plan* plans, int count, const float* bank, int natural, int threads, void* out,
+                      int fp64)
 {
     static float* sinc = NULL;
+    static double* sinc64 = NULL;
     #pragma omp critical(oracle_sinc)
     {
         if (!sinc) {
             float* table = malloc(sizeof(float) * TAPS * (PHASES + 1));
-            sincTable(table);
+            double* wide = malloc(sizeof(double) * TAPS * (PHASES + 1));
+            sincTableBoth(table, wide);
+            sinc64 = wide;
             sinc = table;
         }
     }
@@ -661,6 +690,7 @@ int oracle_synthesize(const cs_plan* plans, int count, const float* bank, int na
     memset(&b, 0, sizeof b);
     b.bank = bank;
     b.sinc = sinc;
+    b.sinc64 = fp64 ? sinc64 : NULL;
     if (buildBatch(&b, plans, count)) {
         freeBatch(&b);
         return 1;
@@ -690,6 +720,21 @@ int oracle_synthesize(const cs_plan* plans, int count, const float* bank, int na
     }
     freeBatch(&b);
     return 0;
+}
+
+/* The batch's mix: float2 per frame (natural) or short2 (orig/custom), jobs
+ * concatenated in plan order. */
+int oracle_synthesize(const cs_plan* plans, int count, const float* bank, int natural, int threads, void* out)
+{
+    return synthesize(plans, count, bank, natural, threads, out, 0);
+}
+
+/* As oracle_synthesize with the resampler in FP64 (interpolateAt64); the rest of
+ * the voice math stays the reference's FP32. */
+int oracle_synthesize_fp64_resampler(const cs_plan* plans, int count, const float* bank, int natural, int threads,
+                                     void* out)
+{
+    return synthesize(plans, count, bank, natural, threads, out, 1);
 }
 
 void oracle_sinc_table(float* out)

@@ -42,6 +42,7 @@ def lib() -> ctypes.CDLL:
         _lib.oracle_finish_stereo.argtypes = [vp, vp, i32, i32, vp, vp]
         if hasattr(_lib, "oracle_synthesize"):
             _lib.oracle_synthesize.argtypes = [vp, i32, vp, i32, i32, vp]
+            _lib.oracle_synthesize_fp64_resampler.argtypes = [vp, i32, vp, i32, i32, vp]
         _lib.oracle_assess.restype = ctypes.c_size_t
         _lib.oracle_assess.argtypes = [vp, i32, vp, i32, vp, i32, vp, vp]
         _lib.oracle_match_group.argtypes = [vp, i32, i32]
@@ -68,14 +69,19 @@ def finish(mix: np.ndarray, plans: list[Plan], natural: bool = True, rate: int =
     return packed[:n], results
 
 
-def synthesize(plans: list[Plan], bank: np.ndarray, natural: bool = True, threads: int = 0) -> np.ndarray:
-    """Restated mix: (frames, 2) float32 in natural mode, int16 otherwise."""
+def synthesize(plans: list[Plan], bank: np.ndarray, natural: bool = True, threads: int = 0,
+               fp64_resampler: bool = False) -> np.ndarray:
+    """Restated mix: (frames, 2) float32 in natural mode, int16 otherwise.  With
+    `fp64_resampler` the 48-tap interpolation runs in FP64 on the unrounded sinc
+    table (the rest of the voice math stays FP32), which bounds the FP32
+    resampler's rounding error independently of the reference's arithmetic."""
     frames = sum(p.frames for p in plans)
     out = np.zeros((frames, 2), np.float32 if natural else np.int16)
     array = c_plans(plans)
     bank = np.ascontiguousarray(bank, np.float32)
-    lib().oracle_synthesize(array, len(plans), bank.ctypes.data if bank.size else None, int(natural),
-                            threads or os.cpu_count() or 1, out.ctypes.data)
+    call = lib().oracle_synthesize_fp64_resampler if fp64_resampler else lib().oracle_synthesize
+    call(array, len(plans), bank.ctypes.data if bank.size else None, int(natural), threads or os.cpu_count() or 1,
+         out.ctypes.data)
     return out
 
 

@@ -86,6 +86,22 @@ def test_uneven_batch_first_64_jobs(uneven_jobs, ref_session):
         np.testing.assert_array_equal(plain_results[field], results[field], err_msg=field)
 
 
+def test_uneven_resampler_against_fp64(uneven_jobs, ref_session):
+    """The GPU render of the first 64 uneven jobs against the oracle with its
+    resampler in FP64 (the unrounded sinc table, double accumulation): the FP32
+    resampler's error, bounded independently of the reference's FP32 arithmetic.
+    The bound is the host FP32-vs-FP64 bound of tests/test_oracle.py plus room for
+    the GPU's contracted envelope and gain arithmetic."""
+    from oracle import oracle
+    from test_oracle import FP64_RESAMPLER_BOUND
+    plans = [ref_session.plan(j.sfz, j.midi) for j in uneven_jobs]
+    bank = ref_session.bank()
+    mix, _, _, _ = render(plans, bank, shared=True)
+    fp64 = oracle.synthesize(plans, bank, fp64_resampler=True)
+    err = np.abs(mix.astype(np.float64) - fp64.astype(np.float64))
+    assert err.max() <= 4 * FP64_RESAMPLER_BOUND, err.max()
+
+
 def test_plain_batch_eight_full_jobs(plain_batch_jobs, ref_session):
     plans = [ref_session.plan(j.sfz, j.midi) for j in plain_batch_jobs]
     assert all(p.filter_tracks > 0 for p in plans)

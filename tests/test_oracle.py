@@ -36,6 +36,29 @@ def test_restated_render_matches_reference_bit_for_bit(request, ref_session, fix
     assert np.array_equal(mine.view(np.uint32 if natural else np.uint16), theirs.view(np.uint32 if natural else np.uint16))
 
 
+# The FP32 resampler (48 FMAs over the FP32-rounded table, render.cu:30-61)
+# against the oracle's FP64 evaluation on the unrounded table
+# (renderer.cpp:365-373): its rounding error, measured on the uneven batch's
+# transposed mono voices, is about 1e-7 FS (a few ULPs at the mix's peak).
+FP64_RESAMPLER_BOUND = 2.5e-7
+
+
+def test_fp64_resampler_bounds_the_fp32_render(tmp_path, ref_session):
+    """The reference's FP32 render (restated bit for bit) of the first 16 jobs of
+    the uneven batch, 87 % of whose voices run the 48-tap sinc, against the same
+    render with the resampler in FP64: the difference is the FP32 resampler's
+    rounding error and stays below FP64_RESAMPLER_BOUND."""
+    from oracle import oracle
+    jobs = workload.write_uneven_batch(tmp_path, seed=2, jobs=1024)[:16]
+    plans = [ref_session.plan(j.sfz, j.midi) for j in jobs]
+    bank = ref_session.bank()
+    fp32 = oracle.synthesize(plans, bank)
+    fp64 = oracle.synthesize(plans, bank, fp64_resampler=True)
+    err = np.abs(fp32.astype(np.float64) - fp64.astype(np.float64))
+    assert 0 < err.max() <= FP64_RESAMPLER_BOUND, err.max()
+    assert np.sqrt(np.mean(err ** 2)) < 1e-8
+
+
 def test_restated_render_pitch_and_bends(tmp_path, ref_session):
     """Variable pitch (LFO to pitch), bends, CC-driven cutoff: the reference's
     check_segments.py voice and check_tail.py's processed preset."""
