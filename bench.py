@@ -522,6 +522,9 @@ def run_b200(args):
         tuned = autotune.tune(plans, bank, device=local, cache=args.workdir / "autotune.json")
         e2e_batch = tuned["batch_jobs"]
     e2e_renderer = Renderer(device=local, natural=True, batch_jobs=e2e_batch)
+    if tuned:
+        e2e_renderer.set_lanes(tuned["lanes"])
+        e2e_renderer.set_shared_sources(tuned["shared_sources"])
     e2e_renderer.upload_samples(bank)
     h2d = sum(p.spans.nbytes + p.points.nbytes + p.modulation.nbytes + p.track_offsets.nbytes for p in plans)
     box = {}

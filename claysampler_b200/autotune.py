@@ -1,19 +1,27 @@
 """Autotuner for the end-to-end render (render_window through the C ABI).
 
-The renderer's kernels have no free shape parameters that keep parity: the tap
-count is fixed at 48, tiles are 256 frames because the tail blocks are 1024
-frames, and every launch covers all of a batch's jobs.  What does change the
-end-to-end rate is how the job list is cut into GPU batches (`batch_jobs`, the
-CLI's --gpu-batch-jobs): larger batches launch fewer, larger grids, while smaller
-ones let the renderer's two stream lanes overlap one batch's upload and download
-with the other's kernels.  The best cut depends on the workload's lengths and on
-its voice mix, so :func:`tune` measures it.  After one discarded warm-up, it
-renders the workload through render_window for every candidate, one untimed pass
-and then `repeats` timed passes, and keeps the candidate whose median pass is
-fastest.  Results are cached per workload signature in
-a JSON file.  Candidates change only the batching, never the audio: publish
-order and PCM are the same for every cut (the renderer's invariant, tested in
-tests/test_serving.py).
+The tap count is fixed at 48 and tiles are 256 frames because the tail blocks
+are 1024 frames, so neither is a free parameter.  What does change the
+end-to-end rate without changing a sample is how the work is cut and overlapped:
+
+* `batch_jobs` (the CLI's --gpu-batch-jobs): how many jobs one GPU batch takes.
+  Larger batches launch fewer, larger grids; smaller ones let the stream lanes
+  overlap one batch's host staging, upload and download with another's kernels.
+* `lanes`: how many batches are in flight at once, each on its own stream lane
+  with its own arena and staging buffers.  More lanes let the host stage the next
+  batches while earlier ones run and download, at the cost of device memory.
+* `shared_sources`: whether each distinct resampled source is rendered once per
+  batch and read by every voice that plays it, or every voice frame is resampled
+  inline.  Which is faster depends on how often sources repeat in a batch.
+
+The best point depends on the workload's lengths and voice mix, so :func:`tune`
+measures it.  After one discarded warm-up, it renders the workload through
+render_window for every candidate, one untimed pass and then `repeats` timed
+passes, and keeps the candidate whose median pass is fastest.  Results are
+cached per workload signature in a JSON file.  Candidates never change the audio:
+publish order and PCM are the same for every cut, lane count and source mode (the
+renderer's invariants, tested in tests/test_serving.py and
+tests/test_gpu_full_size.py).
 """
 from __future__ import annotations
 
@@ -26,7 +34,9 @@ import numpy as np
 
 from .renderer import Renderer
 
-CANDIDATES = (16, 32, 64, 128, 256)
+CANDIDATES = (16, 32, 64, 128, 256, 512)
+LANES = (2, 4)
+SHARED = (True, False)
 RATE = 44100
 
 
@@ -38,10 +48,14 @@ def signature(plans) -> str:
     return h.hexdigest()[:16]
 
 
-def measure(plans, bank, batch_jobs: int, repeats: int = 2, device: int = 0) -> float:
-    """Output audio-seconds per second of render_window with GPU batches of `batch_jobs`."""
+def measure(plans, bank, batch_jobs: int, repeats: int = 2, device: int = 0, lanes: int = 2,
+            shared_sources: bool = True) -> float:
+    """Output audio-seconds per second of render_window with GPU batches of
+    `batch_jobs`, `lanes` batches in flight and shared sources on or off."""
     renderer = Renderer(device=device, natural=True, batch_jobs=batch_jobs)
     try:
+        renderer.set_lanes(lanes)
+        renderer.set_shared_sources(shared_sources)
         renderer.upload_samples(bank)
         audio = [0.0]
 
@@ -61,22 +75,32 @@ def measure(plans, bank, batch_jobs: int, repeats: int = 2, device: int = 0) -> 
 
 
 def tune(plans, bank, candidates=CANDIDATES, repeats: int = 3, device: int = 0,
-         cache: Path | None = None) -> dict:
-    """The fastest GPU batch size for `plans` ({"batch_jobs", "sweep", "signature"})."""
+         cache: Path | None = None, lanes=LANES, shared=SHARED) -> dict:
+    """The fastest render_window settings for `plans`: {"batch_jobs", "lanes",
+    "shared_sources", "sweep", "signature"}.  The batch size is swept first with
+    two lanes and shared sources; the lane counts and the source mode are then
+    tried at the best size."""
     key = signature(plans)
     store = {}
     if cache is not None and cache.exists():
         store = json.loads(cache.read_text())
-        if key in store:
+        if key in store and "lanes" in store[key]:
             return store[key]
     measure(plans, bank, candidates[0], 1, device)        # one-time costs (threads, page-locking) land here
     sweep = {}
     for jobs in candidates:
         if jobs > 2 * len(plans) and sweep:
             break
-        sweep[str(jobs)] = measure(plans, bank, jobs, repeats, device)
-    best = max(sweep, key=sweep.get)
-    result = {"batch_jobs": int(best), "sweep": sweep, "signature": key}
+        sweep[f"{jobs}/2/shared"] = measure(plans, bank, jobs, repeats, device)
+    best_jobs = max(sweep, key=sweep.get).split("/")[0]
+    for count in lanes:
+        for mode in shared:
+            name = f"{best_jobs}/{count}/{'shared' if mode else 'plain'}"
+            if name not in sweep:
+                sweep[name] = measure(plans, bank, int(best_jobs), repeats, device, count, mode)
+    best = max(sweep, key=sweep.get).split("/")
+    result = {"batch_jobs": int(best[0]), "lanes": int(best[1]), "shared_sources": best[2] == "shared",
+              "sweep": sweep, "signature": key}
     if cache is not None:
         store[key] = result
         cache.parent.mkdir(parents=True, exist_ok=True)

@@ -768,9 +768,49 @@ struct MinOp { __device__ int operator()(int a, int b) const { return a < b ? a 
 struct MixVoice {
     long long offset;                   // filtered (shared) + offset + frame * channels is the frame's first sample
     int begin, end, index, kind;        // kind: 0 unfiltered, 1 filtered stereo, 2 filtered mono,
-                                        // 3 shared mono source, 4 shared stereo source
-    int sharedEnd;                      // kinds 3, 4: frames from here on have a silent source
+                                        // 3 shared mono source, 4 shared stereo source, 5 / 6 as 3 / 4
+                                        // with no modulation, no stereo matrix and the tile's pan fixed
+    int sharedEnd;                      // kinds 3-6: frames from here on have a silent source
+    float gainLeft, gainRight;          // kinds 5, 6: the voice's pan gains over the tile
 };
+
+// A job control track (CC7, CC11 or the channel pan) over one 256-frame tile.
+// pointAt never decreases with the frame, so when the tile's first and last
+// frames find the same point every frame between them does too, and the track's
+// value there is that point's line: the expression trackAt evaluates, with the
+// point's fields read once per tile.  Otherwise each frame looks its point up.
+struct TileTrack {
+    float value, step;
+    int frame;                          // the point's frame; INT_MIN: look each frame up
+    int low, high;                      // the track's points
+};
+
+__device__ __forceinline__ TileTrack tileTrackOf(const cs_control_point* __restrict__ points, int low, int high,
+                                                 int first, int last)
+{
+    TileTrack t{0.f, 0.f, INT_MIN, low, high};
+    const int at = pointAt(points, low, high, first);
+    if (at == pointAt(points, low, high, last)) {
+        t.value = __ldg(&points[at].value);
+        t.step = __ldg(&points[at].step);
+        t.frame = __ldg(&points[at].frame);
+    }
+    return t;
+}
+
+__device__ __forceinline__ float tileTrackAt(const TileTrack& t, const cs_control_point* __restrict__ points, int frame)
+{
+    if (t.frame == INT_MIN)
+        return trackAt(points, t.low, t.high, frame);
+    return fmaf(t.step, float(frame - t.frame), t.value);
+}
+
+// Whether a tile track holds one value over [first, last]: a flat line whose
+// point is due at `first`, so every frame adds the same +0 or -0 to its value.
+__device__ __forceinline__ bool tileTrackFixed(const TileTrack& t, int first)
+{
+    return t.frame != INT_MIN && t.step == 0.f && first >= t.frame;
+}
 
 // A tile's voice as the mix reads it (the staged and unstaged paths alike).
 __device__ __forceinline__ MixVoice mixVoiceOf(const BatchView& b, const SegmentView& s, int index)
@@ -781,6 +821,7 @@ __device__ __forceinline__ MixVoice mixVoiceOf(const BatchView& b, const Segment
     m.end = v.end;
     m.index = index;
     m.sharedEnd = 0;
+    m.gainLeft = m.gainRight = 0.f;
     if (v.filterTrack >= 0) {
         m.kind = v.channels == 1 ? 2 : 1;
         m.offset = (long long)s.scratchOffset[index] - (long long)max(v.begin, s.first) * v.channels;
@@ -805,6 +846,14 @@ constexpr int kMixStaged = kMixThreads / kTilesPerBlock;     // staged voices pe
 // general kernel, given more registers for the resampler); 2 when every unfiltered
 // voice reads a shared source; 0 when every voice is filtered.  The lighter
 // kernels keep 64 warps resident.
+//
+// Per tile the CTA stages, before any frame is mixed, the voice list (range,
+// kind, sample offset) and the job's three control tracks (TileTrack), and for
+// shared-source voices without modulation or stereo matrix under a fixed pan,
+// their pan gains: a frame then reads its voice's envelope and source and two
+// staged gains instead of walking bindings and evaluating pan gains, and looks up
+// no track point where the tile sits on one line of each track.  Every value is
+// the one the per-frame expressions give, so the sums are unchanged.
 template <bool Natural, int Inline>
 __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(BatchView b, SegmentView s, StereoStats* stats)
 {
@@ -814,15 +863,22 @@ __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(Ba
     // frame's walk over its voices reads shared memory and then the voice's samples.
     __shared__ MixVoice staged[kTilesPerBlock][kMixStaged];
     __shared__ MixTile tiles[kTilesPerBlock];
+    __shared__ TileTrack tracks[kTilesPerBlock][3];     // CC7, CC11, pan
     __shared__ int mixedTiles;          // bit k: tile k is not all staged stereo filtered voices
-    if (threadIdx.x == 0)
-        mixedTiles = 0;
-    __syncthreads();
     const int block = s.blocks[blockIdx.x];
     const int jobIndex = b.blockJob[block];
     const JobInfo job = b.jobs[jobIndex];
     const int local = block - job.blockFirst;
     const int jobTiles = (job.frames + kTileFrames - 1) / kTileFrames;
+    if (threadIdx.x < kTilesPerBlock * 3) {
+        const int k = int(threadIdx.x) / 3, track = int(threadIdx.x) % 3;
+        const int first = local * kBlockFrames + k * kTileFrames;
+        const int last = min(first + kTileFrames, max(job.frames, first + 1)) - 1;
+        tracks[k][track] = tileTrackOf(b.points, job.tracks[track], job.tracks[track + 1], first, last);
+    }
+    if (threadIdx.x == 0)
+        mixedTiles = 0;
+    __syncthreads();
     {
         const int k = int(threadIdx.x) / kMixStaged, i = int(threadIdx.x) % kMixStaged;
         const int tileIndex = local * kTilesPerBlock + k;
@@ -833,9 +889,21 @@ __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(Ba
                 atomicOr(&mixedTiles, 1 << k);
         }
         if (i < tile.count && tile.count <= kMixStaged) {
-            const MixVoice m = mixVoiceOf(b, s, __ldg(b.indices + tile.first + i));
+            MixVoice m = mixVoiceOf(b, s, __ldg(b.indices + tile.first + i));
             if (m.kind != 1)
                 atomicOr(&mixedTiles, 1 << k);
+            const TileTrack pan = tracks[k][2];
+            const int first = local * kBlockFrames + k * kTileFrames;
+            if (m.kind >= 3) {
+                const cs_voice_span& v = b.voices[m.index];
+                if (v.modulationCount == 0 && !v.stereoMatrix && tileTrackFixed(pan, first)) {
+                    // voiceOutputFrom with no bindings: the pan offset is the track's.
+                    const float2 gains = panGains(v, fmaf(pan.step, float(first - pan.frame), pan.value));
+                    m.gainLeft = gains.x;
+                    m.gainRight = gains.y;
+                    m.kind += 2;
+                }
+            }
             staged[k][i] = m;
         }
     }
@@ -847,7 +915,7 @@ __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(Ba
         if (frame >= job.frames || frame < s.first || frame >= s.end)
             continue;
         const MixTile tile = tiles[k];
-        const float pan = trackAt(b.points, job.tracks[2], job.tracks[3], frame);
+        const float pan = tileTrackAt(tracks[k][2], b.points, frame);
         float left = 0, right = 0, wetLeft = 0, wetRight = 0;
         const auto addVoice = [&](const MixVoice& m) {
             if (frame < m.begin || frame >= m.end)
@@ -874,6 +942,27 @@ __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(Ba
                                                        pan, frame, false, -1.0);
                 left += sample.x;
                 right += sample.y;
+            } else if (Inline && m.kind >= 5) {
+                // voiceFrame with no bindings, its source read from the shared
+                // sources and its pan gains staged for the tile.
+                const float level = envelopeAt(b.voices[m.index], frame);
+                if (level > 0) {
+                    float2 source = make_float2(0.f, 0.f);
+                    if (frame < m.sharedEnd) {
+                        if (m.kind == 5) {
+                            const float x = __ldg(b.shared + (m.offset + frame));
+                            source = make_float2(x, x);
+                        } else {
+                            source = __ldg(reinterpret_cast<const float2*>(b.shared + (m.offset + 2ll * frame)));
+                        }
+                    }
+                    // voiceOutputFrom rounds each product before the sum (its
+                    // result joins other paths), so no multiply-add is fused here.
+                    const float l = source.x * m.gainLeft;
+                    const float r = source.y * m.gainRight;
+                    left += __fmul_rn(l, level);
+                    right += __fmul_rn(r, level);
+                }
             } else if (Inline && m.kind >= 3) {
                 // voiceFrame with the source read from the shared sources.
                 const cs_voice_span& v = b.voices[m.index];
@@ -925,7 +1014,8 @@ __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(Ba
             for (int i = tile.first; i < tile.first + tile.count; ++i)
                 addVoice(mixVoiceOf(b, s, __ldg(b.indices + i)));
         }
-        const float amplitude = jobGainAt(b.points, job.tracks, frame);
+        // CC7 x CC11 (jobGainAt).
+        const float amplitude = tileTrackAt(tracks[k][0], b.points, frame) * tileTrackAt(tracks[k][1], b.points, frame);
         const float x = fmaf(left, amplitude, wetLeft), y = fmaf(right, amplitude, wetRight);
         if (Natural) {
             static_cast<float2*>(b.mix)[job.offset + frame] = make_float2(x, y);
@@ -937,146 +1027,6 @@ __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(Ba
             }
         } else {
             static_cast<short2*>(b.mix)[job.offset + frame] = make_short2(toPcm16(x), toPcm16(y));
-        }
-    }
-    if (Natural) {
-        power = blockReduce(power, 0.0, SumOp{}, reduceD);
-        peak = blockReduce(peak, 0.f, MaxOp{}, reduceF);
-        if (threadIdx.x == 0)
-            stats[block] = {power, peak};
-    }
-}
-
-// The mix of batches whose mix kernel resamples no voice itself (every
-// unfiltered voice reads a shared source, or every voice is filtered).  A CTA per
-// 1024-frame tail block; the 64 threads of each 256-frame tile take four of its
-// frames each, 64 apart (so every warp access stays coalesced), and walk the
-// tile's voices once for all four: a voice's fields are read once per four frames
-// and its four frames are in flight together.  Each frame still adds its voices
-// in span order (renderTiles, render.cu:458-523), so the sums are those of the
-// frame-per-thread mix; the block power and peak are reduced in the same pass
-// (scanStereo, tail.cu:54-81).
-constexpr int kFramesPerThread = kTilesPerBlock;           // 4
-constexpr int kTileThreads = kTileFrames / kFramesPerThread;
-
-template <bool Natural>
-__global__ void __launch_bounds__(kMixThreads, 4) mixSharedKernel(BatchView b, SegmentView s, StereoStats* stats)
-{
-    __shared__ double reduceD[32];
-    __shared__ float reduceF[32];
-    __shared__ MixVoice staged[kTilesPerBlock][kMixStaged];
-    __shared__ MixTile tiles[kTilesPerBlock];
-    const int block = s.blocks[blockIdx.x];
-    const int jobIndex = b.blockJob[block];
-    const JobInfo job = b.jobs[jobIndex];
-    const int local = block - job.blockFirst;
-    const int jobTiles = (job.frames + kTileFrames - 1) / kTileFrames;
-    {
-        const int k = int(threadIdx.x) / kMixStaged, i = int(threadIdx.x) % kMixStaged;
-        const int tileIndex = local * kTilesPerBlock + k;
-        const MixTile tile = tileIndex < jobTiles ? b.tiles[job.tileFirst + tileIndex] : MixTile{0, 0};
-        if (i == 0)
-            tiles[k] = tile;
-        if (i < tile.count && tile.count <= kMixStaged)
-            staged[k][i] = mixVoiceOf(b, s, __ldg(b.indices + tile.first + i));
-    }
-    __syncthreads();
-    const int k = int(threadIdx.x) / kTileThreads, i = int(threadIdx.x) % kTileThreads;
-    const MixTile tile = tiles[k];
-    const int base = local * kBlockFrames + k * kTileFrames + i;
-    int frame[kFramesPerThread];
-    bool live[kFramesPerThread];
-    float pan[kFramesPerThread], left[kFramesPerThread], right[kFramesPerThread];
-    float wetLeft[kFramesPerThread], wetRight[kFramesPerThread];
-    bool any = false;
-    #pragma unroll
-    for (int j = 0; j < kFramesPerThread; ++j) {
-        frame[j] = base + j * kTileThreads;
-        live[j] = frame[j] < job.frames && frame[j] >= s.first && frame[j] < s.end;
-        any |= live[j];
-        pan[j] = live[j] ? trackAt(b.points, job.tracks[2], job.tracks[3], frame[j]) : 0.f;
-        left[j] = right[j] = wetLeft[j] = wetRight[j] = 0.f;
-    }
-    for (int n = 0; any && n < tile.count; ++n) {
-        const MixVoice m = tile.count <= kMixStaged ? staged[k][n] : mixVoiceOf(b, s, __ldg(b.indices + tile.first + n));
-        bool in[kFramesPerThread];
-        bool touched = false;
-        #pragma unroll
-        for (int j = 0; j < kFramesPerThread; ++j) {
-            in[j] = live[j] && frame[j] >= m.begin && frame[j] < m.end;
-            touched |= in[j];
-        }
-        if (!touched)
-            continue;
-        if (m.kind == 1) {
-            #pragma unroll
-            for (int j = 0; j < kFramesPerThread; ++j)
-                if (in[j]) {
-                    const float2 x = *reinterpret_cast<const float2*>(b.filtered + (m.offset + 2ll * frame[j]));
-                    wetLeft[j] += x.x;
-                    wetRight[j] += x.y;
-                }
-        } else if (m.kind == 2) {
-            // Mono filtered voices are panned after the filter.
-            const cs_voice_span& v = b.voices[m.index];
-            #pragma unroll
-            for (int j = 0; j < kFramesPerThread; ++j)
-                if (in[j]) {
-                    const float x = b.filtered[m.offset + frame[j]];
-                    float offset = pan[j];
-                    for (int q = v.firstModulation; q < v.firstModulation + v.modulationCount; ++q) {
-                        const cs_voice_modulation mod = b.modulation[q];
-                        if (mod.target == CS_MOD_PAN)
-                            offset += bindingAt(mod, b.points, frame[j]);
-                    }
-                    const float2 gains = panGains(v, offset);
-                    wetLeft[j] += x * gains.x;
-                    wetRight[j] += x * gains.y;
-                }
-        } else if (m.kind >= 3) {
-            // voiceFrame with the source read from the shared sources.
-            const cs_voice_span& v = b.voices[m.index];
-            #pragma unroll
-            for (int j = 0; j < kFramesPerThread; ++j) {
-                if (!in[j])
-                    continue;
-                const float level = envelopeAt(v, frame[j]);
-                if (level <= 0)
-                    continue;
-                const VoiceMods mods = voiceMods(v, b.points, b.modulation, level, pan[j], frame[j]);
-                float2 source = make_float2(0.f, 0.f);
-                if (frame[j] < m.sharedEnd) {
-                    if (m.kind == 3) {
-                        const float x = __ldg(b.shared + (m.offset + frame[j]));
-                        source = make_float2(x, x);
-                    } else {
-                        source = __ldg(reinterpret_cast<const float2*>(b.shared + (m.offset + 2ll * frame[j])));
-                    }
-                }
-                const float2 out = voiceOutputFrom(source, v, mods, false);
-                left[j] += out.x;
-                right[j] += out.y;
-            }
-        }
-    }
-    double power = 0;
-    float peak = 0;
-    #pragma unroll
-    for (int j = 0; j < kFramesPerThread; ++j) {
-        if (!live[j])
-            continue;
-        const float amplitude = jobGainAt(b.points, job.tracks, frame[j]);
-        const float x = fmaf(left[j], amplitude, wetLeft[j]), y = fmaf(right[j], amplitude, wetRight[j]);
-        if (Natural) {
-            static_cast<float2*>(b.mix)[job.offset + frame[j]] = make_float2(x, y);
-            if (!isfinite(x) || !isfinite(y)) {
-                peak = __int_as_float(0x7f800000);
-            } else {
-                peak = fmaxf(peak, fmaxf(fabsf(x), fabsf(y)));
-                power += double(__fmul_rn(x, x)) + double(__fmul_rn(y, y));
-            }
-        } else {
-            static_cast<short2*>(b.mix)[job.offset + frame[j]] = make_short2(toPcm16(x), toPcm16(y));
         }
     }
     if (Natural) {
@@ -1598,9 +1548,9 @@ void launchMix(const BatchView& b, const SegmentView& s, bool natural, StereoSta
         else
             launch(mixKernel<false, 1>);
     } else if (natural) {
-        launch(mixSharedKernel<true>);
+        launch(mixKernel<true, 2>);
     } else {
-        launch(mixSharedKernel<false>);
+        launch(mixKernel<false, 2>);
     }
 }
 

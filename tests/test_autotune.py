@@ -1,5 +1,6 @@
-"""The end-to-end autotuner: it picks one of its candidate GPU batch sizes, caches
-the choice per workload, and the cut it picks changes no job's audio."""
+"""The end-to-end autotuner: it picks a GPU batch size, a lane count and the
+shared-source mode, caches the choice per workload, and what it picks changes no
+job's audio."""
 import numpy as np
 import pytest
 
@@ -22,12 +23,17 @@ def test_tuned_batching_keeps_every_job_identical(ref_session, batch_mini, plain
     bank = ref_session.bank()
     cache = tmp_path / "autotune.json"
     tuned = autotune.tune(plans, bank, candidates=(1, 2, 8), repeats=1, cache=cache)
-    assert tuned["batch_jobs"] in (1, 2, 8) and set(tuned["sweep"]) == {"1", "2", "8"}
+    assert tuned["batch_jobs"] in (1, 2, 8) and tuned["lanes"] in (2, 4)
+    assert {"1/2/shared", "2/2/shared", "8/2/shared"} <= set(tuned["sweep"])
+    best = tuned["batch_jobs"]
+    assert {f"{best}/2/plain", f"{best}/4/shared", f"{best}/4/plain"} <= set(tuned["sweep"])
     assert all(v > 0 for v in tuned["sweep"].values())
     assert autotune.tune(plans, bank, candidates=(1, 2, 8), cache=cache) == tuned   # cached
 
-    def render(batch_jobs):
+    def render(batch_jobs, lanes=2, shared=True):
         renderer = Renderer(natural=True, batch_jobs=batch_jobs)
+        renderer.set_lanes(lanes)
+        renderer.set_shared_sources(shared)
         renderer.upload_samples(bank)
         jobs = {}
 
@@ -40,7 +46,8 @@ def test_tuned_batching_keeps_every_job_identical(ref_session, batch_mini, plain
         renderer.close()
         return jobs
 
-    one, tuned_jobs = render(1), render(tuned["batch_jobs"])
+    one = render(1, 1, False)
+    tuned_jobs = render(tuned["batch_jobs"], tuned["lanes"], tuned["shared_sources"])
     assert sorted(one) == sorted(tuned_jobs) == list(range(len(plans)))
     for j in one:
         np.testing.assert_array_equal(one[j][0], tuned_jobs[j][0])
