@@ -1207,19 +1207,30 @@ __global__ void __launch_bounds__(kFinalizeWarps * 32) quantizeMonoKernel(BatchV
     if (first >= end)
         return;
     const float scale = result.scale;
-    const float2* mix = static_cast<const float2*>(b.mix) + job.offset;
-    short* mono = f.mono + job.offset;
+    const float2* __restrict__ mix = static_cast<const float2*>(b.mix) + job.offset;
+    short* __restrict__ mono = f.mono + job.offset;
     double power = 0;
     int peak = 0;
-    for (int frame = first + lane; frame < end; frame += 32) {
-        const float2 sample = mix[frame];
-        const int left = __float2int_rn(fminf(32767.f, fmaxf(-32768.f, sample.x * scale)));
-        const int right = __float2int_rn(fminf(32767.f, fmaxf(-32768.f, sample.y * scale)));
-        const int sum = left + right;
-        const int value = (sum >> 1) + ((sum & 1) & ((sum >> 1) & 1));
-        mono[frame] = short(value);
-        power += double(value) * value;
-        peak = max(peak, abs(value));
+    // Each lane takes kUnroll frames 32 apart per step, their loads issued together.
+    constexpr int kUnroll = 4;
+    for (int base = first + lane; base < end; base += 32 * kUnroll) {
+        float2 sample[kUnroll];
+        #pragma unroll
+        for (int u = 0; u < kUnroll; ++u)
+            sample[u] = base + 32 * u < end ? __ldcs(mix + base + 32 * u) : make_float2(0.f, 0.f);
+        #pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const int frame = base + 32 * u;
+            if (frame >= end)
+                break;
+            const int left = __float2int_rn(fminf(32767.f, fmaxf(-32768.f, sample[u].x * scale)));
+            const int right = __float2int_rn(fminf(32767.f, fmaxf(-32768.f, sample[u].y * scale)));
+            const int sum = left + right;
+            const int value = (sum >> 1) + ((sum & 1) & ((sum >> 1) & 1));
+            mono[frame] = short(value);
+            power += double(value) * value;
+            peak = max(peak, abs(value));
+        }
     }
     power = warpAll(power, SumOp{});
     peak = warpAll(peak, MaxOp{});
@@ -1371,32 +1382,48 @@ __global__ void __launch_bounds__(kFinalizeWarps * 32) finalizeKernel(BatchView 
     unsigned long long powerA = 0, powerB = 0;
     int peak = 0, audibleFirst = frames, audibleLast = -1, clipped = 0;
     const int fadeStart = frames - fade;
-    for (int frame = first + lane; frame < end; frame += 32) {
-        int framePeak = 0, mono = 0;
+    const short* __restrict__ source = input + job.offset * Channels;
+    short* __restrict__ packed = f.packed + outputOffset * Channels;
+    // Each lane takes kUnroll frames 32 apart per step, their loads issued together.
+    constexpr int kUnroll = 4;
+    for (int base = first + lane; base < end; base += 32 * kUnroll) {
+        short loaded[kUnroll][Channels];
         #pragma unroll
-        for (int c = 0; c < Channels; ++c) {
-            short value = input[(job.offset + frame) * Channels + c];
-            if (frame >= fadeStart)
-                value = fadeSample(value, frame - fadeStart, fade);
-            f.packed[(outputOffset + frame) * Channels + c] = value;
-            const int magnitude = abs(int(value));
-            framePeak = max(framePeak, magnitude);
-            clipped += magnitude >= 32767;
-            mono += Channels == 1 ? 2 * int(value) : int(value);
-        }
-        peak = max(peak, framePeak);
-        if (framePeak > 3) {
-            audibleFirst = min(audibleFirst, frame);
-            audibleLast = frame;
-        }
-        if (frame < bodyEnd) {
-            const unsigned long long power = (unsigned long long)((long long)mono * mono);
-            if (!paired)
-                atomicAdd(f.bodyPower + bodyFirst + f.body.windowOf(frame), power);
-            else if (frame < split)
-                powerA += power;
-            else
-                powerB += power;
+        for (int u = 0; u < kUnroll; ++u)
+            #pragma unroll
+            for (int c = 0; c < Channels; ++c)
+                loaded[u][c] = base + 32 * u < end ? __ldcs(source + (base + 32 * u) * Channels + c) : short(0);
+        #pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const int frame = base + 32 * u;
+            if (frame >= end)
+                break;
+            int framePeak = 0, mono = 0;
+            #pragma unroll
+            for (int c = 0; c < Channels; ++c) {
+                short value = loaded[u][c];
+                if (frame >= fadeStart)
+                    value = fadeSample(value, frame - fadeStart, fade);
+                packed[frame * Channels + c] = value;
+                const int magnitude = abs(int(value));
+                framePeak = max(framePeak, magnitude);
+                clipped += magnitude >= 32767;
+                mono += Channels == 1 ? 2 * int(value) : int(value);
+            }
+            peak = max(peak, framePeak);
+            if (framePeak > 3) {
+                audibleFirst = min(audibleFirst, frame);
+                audibleLast = frame;
+            }
+            if (frame < bodyEnd) {
+                const unsigned long long power = (unsigned long long)((long long)mono * mono);
+                if (!paired)
+                    atomicAdd(f.bodyPower + bodyFirst + f.body.windowOf(frame), power);
+                else if (frame < split)
+                    powerA += power;
+                else
+                    powerB += power;
+            }
         }
     }
     peak = warpAll(peak, MaxOp{});
