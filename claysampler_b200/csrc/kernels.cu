@@ -772,7 +772,66 @@ struct MixVoice {
                                         // with no modulation, no stereo matrix and the tile's pan fixed
     int sharedEnd;                      // kinds 3-6: frames from here on have a silent source
     float gainLeft, gainRight;          // kinds 5, 6: the voice's pan gains over the tile
+    // Kinds 5, 6: the amplitude envelope's piece over the tile (EnvelopePiece),
+    // the frame it counts from, its rate and its value.
+    int piece, pieceFrame;
+    float pieceRate, pieceValue;
 };
+
+// The pieces of an amplitude envelope (envelopeAt, render.cu:6-19), in the order
+// its tests pick them.  Each piece holds over one interval of frames: a frame's
+// piece follows from comparisons that each flip once as the frame grows, so a
+// tile whose first and last frames share a piece has it for every frame.
+enum EnvelopePiece : int {
+    kPieceStart, kPieceAttack, kPieceHold, kPieceSustain, kPieceDecay, kPieceRelease, kPieceFade, kPieceAny
+};
+
+template <class Shape>
+__device__ __forceinline__ int envelopePiece(const Shape& e, int frame)
+{
+    if (e.releaseStart >= 0 && frame >= e.releaseStart)
+        return frame >= e.fadeStart ? kPieceFade : kPieceRelease;
+    if (frame < e.attackStart) return kPieceStart;
+    if (frame < e.holdStart) return kPieceAttack;
+    if (frame < e.decayStart) return kPieceHold;
+    return e.decayRate == 0 ? kPieceSustain : kPieceDecay;
+}
+
+// Stages the envelope of `m` over frames [first, last] as one piece when it has one.
+template <class Shape>
+__device__ __forceinline__ void stageEnvelope(MixVoice& m, const Shape& e, int first, int last)
+{
+    const int piece = envelopePiece(e, first);
+    m.piece = piece == envelopePiece(e, last) ? piece : kPieceAny;
+    m.pieceFrame = 0;
+    m.pieceRate = m.pieceValue = 0.f;
+    switch (m.piece) {
+    case kPieceStart: m.pieceValue = e.start; break;
+    case kPieceAttack: m.pieceFrame = e.attackStart; m.pieceRate = e.attackStep; m.pieceValue = e.start; break;
+    case kPieceHold: m.pieceValue = 1.f; break;
+    case kPieceSustain: m.pieceValue = e.sustain; break;
+    case kPieceDecay: m.pieceFrame = e.decayStart; m.pieceRate = e.decayRate; m.pieceValue = e.sustain; break;
+    case kPieceRelease:
+        m.pieceFrame = e.releaseStart; m.pieceRate = e.releaseRate; m.pieceValue = e.releaseValue; break;
+    case kPieceFade: m.pieceFrame = e.fadeStart; m.pieceRate = e.fadeStep; m.pieceValue = e.fadeValue; break;
+    default: break;
+    }
+}
+
+// envelopeAt through the staged piece: the same expression on the same fields.
+__device__ __forceinline__ float envelopeOf(const MixVoice& m, const cs_voice_span* __restrict__ voices, int frame)
+{
+    switch (m.piece) {
+    case kPieceStart:
+    case kPieceHold:
+    case kPieceSustain: return m.pieceValue;
+    case kPieceAttack: return fminf(1.f, m.pieceValue + float(frame - m.pieceFrame + 1) * m.pieceRate);
+    case kPieceDecay: return fmaxf(m.pieceValue, expf(float(frame - m.pieceFrame + 1) * m.pieceRate));
+    case kPieceRelease: return m.pieceValue * expf(float(frame - m.pieceFrame + 1) * m.pieceRate);
+    case kPieceFade: return fmaxf(0.f, m.pieceValue - float(frame - m.pieceFrame + 1) * m.pieceRate);
+    default: return envelopeAt(voices[m.index], frame);
+    }
+}
 
 // A job control track (CC7, CC11 or the channel pan) over one 256-frame tile.
 // pointAt never decreases with the frame, so when the tile's first and last
@@ -822,6 +881,7 @@ __device__ __forceinline__ MixVoice mixVoiceOf(const BatchView& b, const Segment
     m.index = index;
     m.sharedEnd = 0;
     m.gainLeft = m.gainRight = 0.f;
+    m.piece = kPieceAny;
     if (v.filterTrack >= 0) {
         m.kind = v.channels == 1 ? 2 : 1;
         m.offset = (long long)s.scratchOffset[index] - (long long)max(v.begin, s.first) * v.channels;
@@ -902,6 +962,8 @@ __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(Ba
                     m.gainLeft = gains.x;
                     m.gainRight = gains.y;
                     m.kind += 2;
+                    const int last = min(first + kTileFrames, max(job.frames, first + 1)) - 1;
+                    stageEnvelope(m, v, max(first, m.begin), min(last, m.end - 1));
                 }
             }
             staged[k][i] = m;
@@ -944,8 +1006,8 @@ __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(Ba
                 right += sample.y;
             } else if (Inline && m.kind >= 5) {
                 // voiceFrame with no bindings, its source read from the shared
-                // sources and its pan gains staged for the tile.
-                const float level = envelopeAt(b.voices[m.index], frame);
+                // sources and its pan gains and envelope piece staged for the tile.
+                const float level = envelopeOf(m, b.voices, frame);
                 if (level > 0) {
                     float2 source = make_float2(0.f, 0.f);
                     if (frame < m.sharedEnd) {
