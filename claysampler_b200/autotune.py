@@ -32,6 +32,7 @@ from pathlib import Path
 
 import numpy as np
 
+from .plans import PlanSet
 from .renderer import Renderer
 
 CANDIDATES = (16, 32, 64, 128, 256, 512)
@@ -52,6 +53,7 @@ def measure(plans, bank, batch_jobs: int, repeats: int = 2, device: int = 0, lan
             shared_sources: bool = True) -> float:
     """Output audio-seconds per second of render_window with GPU batches of
     `batch_jobs`, `lanes` batches in flight and shared sources on or off."""
+    plans = plans if isinstance(plans, PlanSet) else PlanSet(plans)
     renderer = Renderer(device=device, natural=True, batch_jobs=batch_jobs)
     try:
         renderer.set_lanes(lanes)
@@ -79,7 +81,7 @@ def tune(plans, bank, candidates=CANDIDATES, repeats: int = 3, device: int = 0,
     """The fastest render_window settings for `plans`: {"batch_jobs", "lanes",
     "shared_sources", "sweep", "signature"}.  The batch size is swept first with
     two lanes and shared sources; the lane counts and the source mode are then
-    tried at the best size."""
+    tried at the two best sizes."""
     key = signature(plans)
     store = {}
     if cache is not None and cache.exists():
@@ -92,12 +94,15 @@ def tune(plans, bank, candidates=CANDIDATES, repeats: int = 3, device: int = 0,
         if jobs > 2 * len(plans) and sweep:
             break
         sweep[f"{jobs}/2/shared"] = measure(plans, bank, jobs, repeats, device)
-    best_jobs = max(sweep, key=sweep.get).split("/")[0]
-    for count in lanes:
-        for mode in shared:
-            name = f"{best_jobs}/{count}/{'shared' if mode else 'plain'}"
-            if name not in sweep:
-                sweep[name] = measure(plans, bank, int(best_jobs), repeats, device, count, mode)
+    # Lanes and source mode at the two fastest batch sizes (neighbours often
+    # trade places once more batches overlap).
+    leaders = sorted(sweep, key=sweep.get, reverse=True)[:2]
+    for best_jobs in (name.split("/")[0] for name in leaders):
+        for count in lanes:
+            for mode in shared:
+                name = f"{best_jobs}/{count}/{'shared' if mode else 'plain'}"
+                if name not in sweep:
+                    sweep[name] = measure(plans, bank, int(best_jobs), repeats, device, count, mode)
     best = max(sweep, key=sweep.get).split("/")
     result = {"batch_jobs": int(best[0]), "lanes": int(best[1]), "shared_sources": best[2] == "shared",
               "sweep": sweep, "signature": key}

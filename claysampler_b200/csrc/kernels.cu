@@ -1512,6 +1512,135 @@ __global__ void __launch_bounds__(kFinalizeWarps * 32) finalizeKernel(BatchView 
     }
 }
 
+// ---- mix tile voice lists ---------------------------------------------------------------
+//
+// The voice list of a 256-frame tile holds the job's spans that overlap it, in
+// span order (the reference's BatchIndex::append, src/cuda/renderer.cpp:390-460).
+// A CTA per (job, chunk of kIndexChunkTiles tiles).  The CTA first gathers, in
+// span order, the job's spans that overlap the chunk into shared memory (an
+// order-keeping compaction per 256 spans) and sums the entries of the job's
+// earlier chunks; then each thread owns eight consecutive tiles of the chunk and
+// walks the gathered spans in order twice, to count its tiles' voices and to
+// write their lists, so each list comes out in span order and no two threads
+// write the same slot.  A chunk overlapped by more spans than the shared list
+// holds walks the job's spans in global memory instead.
+constexpr int kIndexThreads = kIndexChunkTiles / 8;
+constexpr int kIndexList = 2048;
+
+__global__ void __launch_bounds__(kIndexThreads) tileIndexKernel(BatchView b, const JobSpans* __restrict__ spans,
+                                                                 const int2* __restrict__ units, MixTile* tiles,
+                                                                 int* indices)
+{
+    __shared__ int listSpan[kIndexList], listFirst[kIndexList], listLast[kIndexList];
+    __shared__ int warpCount[kIndexThreads / 32], warpSum[kIndexThreads / 32];
+    __shared__ int listed;
+    const int2 unit = units[blockIdx.x];
+    const JobInfo job = b.jobs[unit.x];
+    const JobSpans js = spans[unit.x];
+    const int jobTiles = (job.frames + kTileFrames - 1) / kTileFrames;
+    const int chunkFirst = unit.y * kIndexChunkTiles, chunkLast = chunkFirst + kIndexChunkTiles - 1;
+    const int lane = int(threadIdx.x & 31), warp = int(threadIdx.x >> 5);
+    if (threadIdx.x == 0)
+        listed = 0;
+    __syncthreads();
+    int before = 0;                     // entries below the chunk of this thread's spans
+    for (int round = 0; round < js.voiceCount; round += kIndexThreads) {
+        const int k = round + int(threadIdx.x);
+        int a = 0, e = -1;
+        if (k < js.voiceCount) {
+            const cs_voice_span& v = b.voices[js.voiceFirst + k];
+            a = v.begin / kTileFrames;
+            e = (v.end - 1) / kTileFrames;
+            before += max(0, min(e, chunkFirst - 1) - a + 1);
+        }
+        const bool overlaps = k < js.voiceCount && e >= chunkFirst && a <= chunkLast;
+        const unsigned ballot = __ballot_sync(0xffffffffu, overlaps);
+        if (lane == 0)
+            warpCount[warp] = __popc(ballot);
+        __syncthreads();
+        int at = listed + __popc(ballot & ((1u << lane) - 1));
+        for (int w = 0; w < warp; ++w)
+            at += warpCount[w];
+        if (overlaps && at < kIndexList) {
+            listSpan[at] = k;
+            listFirst[at] = a;
+            listLast[at] = e;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (int w = 0; w < kIndexThreads / 32; ++w)
+                listed += warpCount[w];
+        __syncthreads();
+    }
+    const bool inShared = listed <= kIndexList;
+    const int candidates = inShared ? listed : js.voiceCount;
+    const auto spanAt = [&](int i, int& k, int& a, int& e) {
+        if (inShared) {
+            k = listSpan[i];
+            a = listFirst[i];
+            e = listLast[i];
+        } else {
+            const cs_voice_span& v = b.voices[js.voiceFirst + i];
+            k = i;
+            a = v.begin / kTileFrames;
+            e = (v.end - 1) / kTileFrames;
+        }
+    };
+    const int first = chunkFirst + int(threadIdx.x) * 8;       // this thread's first tile
+    int count[8] = {};
+    for (int i = 0; i < candidates; ++i) {
+        int k, a, e;
+        spanAt(i, k, a, e);
+        #pragma unroll
+        for (int j = 0; j < 8; ++j)
+            count[j] += first + j >= a && first + j <= e;
+    }
+    int own = 0;
+    #pragma unroll
+    for (int j = 0; j < 8; ++j)
+        own += count[j];
+    // Exclusive scan of the threads' entries in tile order, and the sum of `before`.
+    int inclusive = own, total = before;
+    #pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int up = __shfl_up_sync(0xffffffffu, inclusive, d);
+        if (lane >= d)
+            inclusive += up;
+        total += __shfl_xor_sync(0xffffffffu, total, d);
+    }
+    if (lane == 31)
+        warpCount[warp] = inclusive;
+    if (lane == 0)
+        warpSum[warp] = total;
+    __syncthreads();
+    int offset = js.indexFirst + inclusive - own;
+    for (int w = 0; w < kIndexThreads / 32; ++w) {
+        offset += warpSum[w];
+        if (w < warp)
+            offset += warpCount[w];
+    }
+    int cursor[8];
+    #pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        cursor[j] = offset;
+        if (first + j < jobTiles)
+            tiles[job.tileFirst + first + j] = MixTile{offset, count[j]};
+        offset += count[j];
+    }
+    if (!own)
+        return;
+    for (int i = 0; i < candidates; ++i) {
+        int k, a, e;
+        spanAt(i, k, a, e);
+        if (e < first || a > first + 7)
+            continue;
+        #pragma unroll
+        for (int j = 0; j < 8; ++j)
+            if (first + j >= a && first + j <= e)
+                indices[cursor[j]++] = js.voiceFirst + k;
+    }
+}
+
 // ---- launchers --------------------------------------------------------------------------
 
 __global__ void expandTilesKernel(const int4* runs, int count, int2* tiles)
@@ -1618,6 +1747,13 @@ int launchGeneralChains(const BatchView& b, const SegmentView& s, cudaStream_t s
 // The inline mix kernels need about 33 KB of shared memory per SM (five CTAs); the
 // rest of the SM's 256 KB goes to L1, where the 393 KB sinc table competes for room.
 constexpr int kInlineMixCarveout = 20;
+
+void launchTileIndex(const BatchView& b, const JobSpans* spans, const int2* units, int unitCount, MixTile* tiles,
+                     int* indices, cudaStream_t stream)
+{
+    if (unitCount)
+        tileIndexKernel<<<unitCount, kIndexThreads, 0, stream>>>(b, spans, units, tiles, indices);
+}
 
 void launchMix(const BatchView& b, const SegmentView& s, bool natural, StereoStats* stats, cudaStream_t stream)
 {

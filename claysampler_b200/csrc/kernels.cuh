@@ -30,13 +30,25 @@ constexpr int kRecChunkFrames = 32;
 // Host phases of staging a batch, timed per renderer: index building, scratch
 // budget, segment planning, shared-source planning, arena, staging pieces,
 // staging copies and upload issue, upload wait.
-constexpr int kHostPhases = 8;
+constexpr int kHostPhases = 10;
+// The last two entries of the staging-time counters are device times of the
+// published batches: their download copies and their kernels.
+constexpr int kPhaseDownload = 8, kPhaseKernels = 9;
 
 // A mix tile: kTileFrames frames of one job with the spans that overlap it
 // (the reference's Tile, src/cuda/render_types.h:70-74).
 struct MixTile {
     int first, count;                   // range in the voice index list
 };
+
+// A job's spans in the batch and where its tile voice lists start in the batch's
+// index list (tileIndexKernel builds the lists on the device).
+struct JobSpans {
+    int voiceFirst, voiceCount, indexFirst, unused;
+};
+
+// Tiles of a job that one tileIndexKernel CTA lists.
+constexpr int kIndexChunkTiles = 2048;
 
 struct JobInfo {
     uint64_t offset;                    // first frame of the job in the batch mix
@@ -202,6 +214,11 @@ void launchScan(const BatchView& b, StereoStats* stats, int blocks, cudaStream_t
 // (span, first frame, end frame, first tile).
 void launchExpandTiles(const int4* runs, int count, int2* tiles, cudaStream_t stream);
 void launchPitch(const BatchView& b, const SegmentView& s, cudaStream_t stream);
+// The mix tiles' voice lists: for each unit (job, chunk of kIndexChunkTiles tiles)
+// the tiles' ranges into `indices` and, per tile, the job's overlapping spans in
+// span order.
+void launchTileIndex(const BatchView& b, const JobSpans* spans, const int2* units, int unitCount, MixTile* tiles,
+                     int* indices, cudaStream_t stream);
 // Renders the shared voice sources: `tiles` holds (source, first frame) every
 // kSourceTile frames.
 int launchSharedSources(const BatchView& b, const SharedSource* sources, const int2* tiles, int tileCount,

@@ -69,8 +69,12 @@ struct HostBatch {
     size_t pointCount = 0;
     std::vector<cs_voice_modulation> modulation;
     std::vector<JobInfo> jobs;
-    std::vector<MixTile> tiles;
-    std::vector<int> indices, blockJob, windowJob, chainHeads, pitchHeads, jobBlockFirst;
+    // The mix tiles' voice lists are built on the device (tileIndexKernel) from
+    // each job's spans and index base, one unit per (job, chunk of tiles).
+    std::vector<JobSpans> jobSpans;
+    std::vector<int2> indexUnits;
+    size_t tileCount = 0, indexCount = 0;
+    std::vector<int> blockJob, windowJob, chainHeads, pitchHeads, jobBlockFirst;
     size_t frames = 0;
     int blocks = 0, windows = 0, lastFrame = 0;
     // Quality gate / group volume inputs (src/cuda/renderer.cpp:801-842).
@@ -128,8 +132,15 @@ struct HostBatch {
             throw std::runtime_error("batch too large for 32-bit indices");
         voices.resize(next.voice);
         modulation.resize(next.modulation);
-        tiles.resize(next.tile);
-        indices.resize(next.index);
+        tileCount = next.tile;
+        indexCount = next.index;
+        jobSpans.resize(count);
+        indexUnits.clear();
+        for (size_t j = 0; j < count; ++j) {
+            const int chunks = int((at[j + 1].tile - at[j].tile + kIndexChunkTiles - 1) / kIndexChunkTiles);
+            for (int c = 0; c < chunks; ++c)
+                indexUnits.push_back(make_int2(int(j), c));
+        }
         blockJob.resize(next.block);
         windowJob.resize(next.window);
         jobs.resize(count);
@@ -174,28 +185,11 @@ struct HostBatch {
                 }
                 modulation[base.modulation + size_t(m)] = binding;
             }
-            // Voice lists per tile via a difference array over tile indices.
-            const int tileCount = (plan.frames + kTileFrames - 1) / kTileFrames;
-            std::vector<int> counts(size_t(tileCount) + 1, 0);
-            for (int k = 0; k < plan.span_count; ++k) {
-                const auto& span = plan.spans[k];
-                ++counts[size_t(span.begin / kTileFrames)];
-                --counts[size_t((span.end - 1) / kTileFrames + 1)];
-            }
-            std::partial_sum(counts.begin(), counts.end(), counts.begin());
-            std::vector<int> cursor(static_cast<size_t>(tileCount), 0);
-            int indexCount = int(base.index);
-            for (int t = 0; t < tileCount; ++t) {
-                tiles[base.tile + size_t(t)] = {indexCount, counts[size_t(t)]};
-                cursor[size_t(t)] = indexCount;
-                indexCount += counts[size_t(t)];
-            }
+            jobSpans[j] = JobSpans{int(base.voice), plan.span_count, int(base.index), 0};
             std::vector<int> chainTail(size_t(plan.filter_tracks), -1);
             for (int k = 0; k < plan.span_count; ++k) {
                 cs_voice_span voice = plan.spans[k];
                 const int index = int(base.voice) + k;
-                for (int t = voice.begin / kTileFrames; t <= (voice.end - 1) / kTileFrames; ++t)
-                    indices[size_t(cursor[size_t(t)]++)] = index;
                 voice.firstModulation += int(base.modulation);
                 if (voice.filterTrack >= 0) {
                     int& tail = chainTail[size_t(voice.filterTrack)];
@@ -710,6 +704,8 @@ struct cs_prepared {
     cs::SegmentTables tables;
     cs::SharedPlan shared;              // shared voice sources (empty: every source inline)
     const cs::SharedSource* sharedSources = nullptr;
+    const cs::JobSpans* jobSpans = nullptr;       // device: the tile index inputs
+    const int2* indexUnits = nullptr;
     const int2* sharedTiles = nullptr;
     void* arena = nullptr;
     size_t arenaBytes = 0;
@@ -736,6 +732,7 @@ struct cs_prepared {
     // buffer (error flag, results, PCM up to the batch's frames), done at `copied`.
     bool asyncDownload = false;
     cudaEvent_t copied = nullptr;
+    cudaEvent_t downloading = nullptr;  // recorded before the download copies
     size_t downloadResults = 0, downloadPcm = 0;   // offsets in the lane's buffer
     // Optional per-stage timing: an event after every stage of the last run.
     bool profile = false;
@@ -919,8 +916,8 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     const size_t oPoints = section(batch.pointCount * sizeof(cs_control_point));
     const size_t oMods = section(batch.modulation.size() * sizeof(cs_voice_modulation));
     const size_t oJobs = section(jobs * sizeof(JobInfo));
-    const size_t oTiles = section(batch.tiles.size() * sizeof(MixTile));
-    const size_t oIndices = section(batch.indices.size() * sizeof(int));
+    const size_t oJobSpans = section(batch.jobSpans.size() * sizeof(JobSpans));
+    const size_t oIndexUnits = section(batch.indexUnits.size() * sizeof(int2));
     const size_t oBlockJob = section(batch.blockJob.size() * sizeof(int));
     const size_t oWindowJob = section(batch.windowJob.size() * sizeof(int));
     const size_t oScratchOff = section(t.scratchOffset.size() * sizeof(uint64_t));
@@ -942,6 +939,8 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     const size_t uploadEnd = layout.bytes;
     p->stateBytes = batch.voices.size() * sizeof(ChainState);
     const size_t oStates = section(p->stateBytes);
+    const size_t oTiles = section(batch.tileCount * sizeof(MixTile));
+    const size_t oIndices = section(batch.indexCount * sizeof(int));
     p->resultBytes = jobs * sizeof(cs_tail_result);
     const size_t oResults = section(p->resultBytes);
     const size_t oScans = section(jobs * sizeof(JobScan));
@@ -1031,8 +1030,8 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     }
     stage(oMods, batch.modulation);
     stage(oJobs, batch.jobs);
-    stage(oTiles, batch.tiles);
-    stage(oIndices, batch.indices);
+    stage(oJobSpans, batch.jobSpans);
+    stage(oIndexUnits, batch.indexUnits);
     stage(oBlockJob, batch.blockJob);
     stage(oWindowJob, batch.windowJob);
     stage(oScratchOff, t.scratchOffset);
@@ -1114,6 +1113,8 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     v.blockJob = reinterpret_cast<const int*>(base + oBlockJob);
     v.windowJob = reinterpret_cast<const int*>(base + oWindowJob);
     v.states = reinterpret_cast<ChainState*>(base + oStates);
+    p->jobSpans = reinterpret_cast<const JobSpans*>(base + oJobSpans);
+    p->indexUnits = reinterpret_cast<const int2*>(base + oIndexUnits);
     v.filtered = reinterpret_cast<float*>(base + oScratch);
     v.mix = base + oMix;
     v.error = reinterpret_cast<int*>(base + oError);
@@ -1201,8 +1202,9 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     return p.release();
 }
 
-const char* const kStageNames[] = {"pitch", "source", "recurrence", "general", "mix", "finish", "assess", "shared"};
-constexpr int kStages = 8;
+const char* const kStageNames[] = {"pitch", "source", "recurrence", "general", "mix", "finish", "assess", "shared",
+                                   "index"};
+constexpr int kStages = 9;
 
 void run(cs_renderer& r, cs_prepared& p, cudaStream_t stream)
 {
@@ -1232,6 +1234,10 @@ void run(cs_renderer& r, cs_prepared& p, cudaStream_t stream)
     if (p.bodyBytes)
         check(cudaMemsetAsync(p.finish.bodyPower, 0, p.bodyBytes, stream), "CUDA body power reset");
     stage(-1);
+    launchTileIndex(p.view, p.jobSpans, p.indexUnits, int(p.batch.indexUnits.size()), const_cast<MixTile*>(p.view.tiles),
+                    const_cast<int*>(p.view.indices), stream);
+    launches += p.batch.indexUnits.empty() ? 0 : 1;
+    stage(8);
     launches += launchSharedSources(p.view, p.sharedSources, p.sharedTiles, int(p.shared.tiles), stream);
     stage(7);
     for (size_t i = 0; i < p.segments.size(); ++i) {
@@ -1333,7 +1339,10 @@ void enqueueDownload(cs_renderer& r, cs_prepared& p)
     auto* buffer = static_cast<unsigned char*>(
         cs_renderer::pinned(lane.download, lane.downloadCapacity, p.downloadPcm + std::max<size_t>(pcmBytes, 1)));
     if (!p.copied)
-        check(cudaEventCreateWithFlags(&p.copied, cudaEventDisableTiming), "CUDA download event");
+        check(cudaEventCreate(&p.copied), "CUDA download event");
+    if (!p.downloading)
+        check(cudaEventCreate(&p.downloading), "CUDA download event");
+    check(cudaEventRecord(p.downloading, lane.stream), "CUDA download event");
     check(cudaMemcpyAsync(buffer, p.view.error, sizeof(int), cudaMemcpyDeviceToHost, lane.stream), "CUDA error flag download");
     check(cudaMemcpyAsync(buffer + p.downloadResults, p.finish.results, p.resultBytes, cudaMemcpyDeviceToHost, lane.stream),
           "CUDA render metadata download");
@@ -1781,6 +1790,10 @@ private:
     {
         if (p.asyncDownload) {
             check(cudaEventSynchronize(p.copied), "CUDA batch download");
+            float copyMs = 0;
+            if (cudaEventElapsedTime(&copyMs, p.downloading, p.copied) == cudaSuccess)
+                r.hostMs[kPhaseDownload] += copyMs;
+            r.hostMs[kPhaseKernels] += 1e3 * seconds(p);
             const auto* buffer = static_cast<const unsigned char*>(r.lanes[p.lane].download);
             int failed = 0;
             std::memcpy(&failed, buffer, sizeof(int));
@@ -2214,6 +2227,7 @@ void cs_prepared_destroy(cs_prepared* p)
     if (p->begin) cudaEventDestroy(p->begin);
     if (p->end) cudaEventDestroy(p->end);
     if (p->copied) cudaEventDestroy(p->copied);
+    if (p->downloading) cudaEventDestroy(p->downloading);
     if (p->arena && !p->sharedArena) {
         cudaFree(p->arena);
         if (p->owner)

@@ -139,25 +139,52 @@ class Plan:
     def track(self, index: int) -> np.ndarray:
         return self.points[self.track_offsets[index]:self.track_offsets[index + 1]]
 
+    def _c_key(self) -> tuple:
+        return (id(self.spans), id(self.points), id(self.track_offsets), id(self.modulation), id(self.onsets),
+                self.filter_tracks, self.frames, self.music_end, self.limit, self.fade_frames, self.tail_clipped,
+                self.body_frames, self.volume_group)
+
     def as_c(self) -> CPlan:
+        """The plan as a ``cs_plan`` view of its arrays, cached until a field or an
+        array of the plan is replaced (the cache holds the arrays it points to)."""
+        key = self._c_key()
+        cached = self.__dict__.get("_c")
+        if cached is not None and cached[0] == key:
+            return cached[1]
         arrays = [np.ascontiguousarray(a) for a in (self.spans, self.points, self.track_offsets.astype(np.int64),
                                                     self.modulation, self.onsets.astype(np.int32))]
-        self._keep = arrays
         ptr = [a.ctypes.data if a.size else None for a in arrays]
-        return CPlan(ptr[0], ptr[1], ptr[2], ptr[3], ptr[4], len(self.spans), self.track_count,
+        view = CPlan(ptr[0], ptr[1], ptr[2], ptr[3], ptr[4], len(self.spans), self.track_count,
                      len(self.modulation), len(self.onsets), self.filter_tracks, self.frames, self.music_end,
                      self.limit, self.fade_frames, self.tail_clipped, self.body_frames, self.volume_group)
+        self._keep = arrays
+        self._c = (key, view)
+        return view
 
     def voice_frames(self) -> int:
         return int(np.sum(self.spans["end"].astype(np.int64) - self.spans["begin"]))
 
 
+class PlanSet(tuple):
+    """An immutable sequence of plans with its ``cs_plan`` array built once, for
+    callers that render the same plans repeatedly (as a C caller keeps its plan
+    array); the renderer's calls take it wherever they take a list of plans."""
+
+    def __new__(cls, plans=()):
+        self = super().__new__(cls, plans)
+        self.array = _build_array(self)
+        return self
+
+
+def _build_array(plans):
+    return (CPlan * len(plans))(*[plan.as_c() for plan in plans])
+
+
 def c_plans(plans: list[Plan]):
     """A ctypes array of ``cs_plan`` views (the plans keep their buffers alive)."""
-    array = (CPlan * len(plans))()
-    for i, plan in enumerate(plans):
-        array[i] = plan.as_c()
-    return array
+    if isinstance(plans, PlanSet):
+        return plans.array
+    return _build_array(plans)
 
 
 def default_audio_config(rate: int = 44100, quality: bool = False) -> np.ndarray:

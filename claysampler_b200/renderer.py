@@ -248,10 +248,12 @@ class Renderer:
         return int(library().cs_renderer_deferred_launches(self.handle))
 
     def host_ms(self) -> dict[str, float]:
-        """Host milliseconds spent staging batches so far, per phase."""
+        """Host milliseconds spent staging batches so far, per phase, then the device
+        milliseconds of the published batches' downloads and kernels."""
         out = (ctypes.c_double * 16)()
         count = library().cs_renderer_host_ms(self.handle, out, 16)
-        names = ("index", "budget", "segments", "shared", "arena", "pieces", "copy", "wait")
+        names = ("index", "budget", "segments", "shared", "arena", "pieces", "copy", "wait", "d2h_device",
+                 "kernels_device")
         return {names[i] if i < len(names) else str(i): float(out[i]) for i in range(count)}
 
     def set_shared_sources(self, enable: bool) -> None:

@@ -274,8 +274,10 @@ int cs_renderer_set_scratch_limit(cs_renderer* renderer, size_t bytes);
 int cs_renderer_set_shared_sources(cs_renderer* renderer, int enable);
 /* Host milliseconds the renderer spent staging batches so far, per phase: batch
  * index (voices, tiles, jobs), scratch budget, segment plan, shared-source plan,
- * arena, staging pieces, staging copies and upload issue, upload wait.  Writes up to `capacity` values and returns the phase count.  No
- * counterpart in the reference. */
+ * arena, staging pieces, staging copies and upload issue, upload wait; then two
+ * device times of the batches render_window / cs_poll published: their download
+ * copies and their kernels.  Writes up to `capacity` values and returns the count.
+ * No counterpart in the reference. */
 int cs_renderer_host_ms(const cs_renderer* renderer, double* ms, int capacity);
 /* Batches in flight at most (1-4, default 2), each on its own stream lane with its
  * own arena.  cs_render_window publishes batches in order; cs_poll publishes them

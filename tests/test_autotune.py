@@ -26,7 +26,7 @@ def test_tuned_batching_keeps_every_job_identical(ref_session, batch_mini, plain
     assert tuned["batch_jobs"] in (1, 2, 8) and tuned["lanes"] in (2, 4)
     assert {"1/2/shared", "2/2/shared", "8/2/shared"} <= set(tuned["sweep"])
     best = tuned["batch_jobs"]
-    assert {f"{best}/2/plain", f"{best}/4/shared", f"{best}/4/plain"} <= set(tuned["sweep"])
+    assert {f"{best}/2/shared", f"{best}/2/plain", f"{best}/4/shared", f"{best}/4/plain"} <= set(tuned["sweep"])
     assert all(v > 0 for v in tuned["sweep"].values())
     assert autotune.tune(plans, bank, candidates=(1, 2, 8), cache=cache) == tuned   # cached
 
