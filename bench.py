@@ -268,16 +268,17 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def traffic_per_unit():
-    """DRAM bytes per voice-frame per kernel from the committed ncu summary."""
+def traffic_per_unit(workload_name: str) -> dict:
+    """DRAM bytes per voice-frame per kernel for `workload_name` from the committed
+    ncu summary (rows: workload, kernel, bytes per voice-frame, algorithmic bytes)."""
     path = ROOT / "profiles" / "dram_traffic.txt"
     table = {}
     if path.exists():
         for line in path.read_text().splitlines():
             parts = line.split()
-            if len(parts) >= 2 and not line.startswith("#"):
+            if len(parts) >= 3 and not line.startswith("#") and parts[0] == workload_name:
                 try:
-                    table[parts[0]] = float(parts[1])
+                    table[parts[1]] = float(parts[2])
                 except ValueError:
                     pass
     return table
@@ -568,7 +569,7 @@ def run_b200(args):
         candidates = {k: stage_ms.get(k, 0.0) for k in ("source", "recurrence", "mix", "shared")}
         dominant = max(candidates, key=candidates.get)
         achieved = algorithmic[dominant] / (stage_ms[dominant] * 1e-3) / 1e9
-        per_unit = traffic_per_unit()
+        per_unit = traffic_per_unit(args.workload)
         voice_frames = sum(p.voice_frames() for p in plans)
         traffic = per_unit[dominant] * voice_frames if dominant in per_unit else None
         clock = clocks.summary().get("sm_mhz") or 1965.0

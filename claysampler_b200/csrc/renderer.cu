@@ -557,8 +557,11 @@ struct SharedPlan {
 bool resamples(const cs_voice_span& v) { return v.step != 1.0 || v.pitchSlope != 0; }
 
 // The first elapsed frame at which a voice without loop or pitch ramp is past
-// its sample's end, with the device's double arithmetic (position + elapsed x step,
-// multiplied and added separately); every later frame is past it as well.
+// its sample's end in the device's double arithmetic, position + elapsed x step,
+// whether the compiler fuses the multiply-add or not (the frame both forms put
+// past the end); every later frame is past it as well.  The frames before it are
+// rendered into the shared source, so a frame one form still finds inside the
+// sample is never dropped.
 long long silentFrom(const cs_voice_span& v)
 {
     const double span = double(v.sourceEnd) - v.position;
@@ -566,8 +569,9 @@ long long silentFrom(const cs_voice_span& v)
     for (;;) {
         const double distance = double(e);
         const double product = distance * v.step;
-        const double pos = v.position + product;
-        if (pos >= double(v.sourceEnd))
+        const double separate = v.position + product;
+        const double fused = std::fma(distance, v.step, v.position);
+        if (separate >= double(v.sourceEnd) && fused >= double(v.sourceEnd))
             return e;
         ++e;
     }
