@@ -712,23 +712,41 @@ __global__ void __launch_bounds__(kRecThreads, 1) recurrenceKernel(BatchView b, 
 
 // ---- shared voice sources ------------------------------------------------------------
 //
-// One CTA per 256-frame tile of a shared source, a thread per frame: the voice
-// source of render.cu:63-100 (position, loop wrap and crossfade, 48-tap sinc) at
-// the elapsed frame, stored as one float (mono) or two (stereo).  The mix then
-// reads it for every voice that plays the source.
-__global__ void __launch_bounds__(kSourceThreads) sharedSourceKernel(BatchView b, const SharedSource* __restrict__ sources,
-                                                                     const int2* __restrict__ tiles)
+// The voice source of render.cu:63-100 (position, loop wrap and crossfade, 48-tap
+// sinc) of every frame of every shared source, stored as one float (mono) or two
+// (stereo); the mix then reads it for every voice that plays the source.  A
+// persistent CTA per SM first copies the half sinc table (phases 0-1024, 213 KB)
+// into shared memory, where each lane's scattered row reads cost a shared-memory
+// access instead of an L2 round trip, then takes 256-frame tiles, a thread per
+// frame, consecutive threads on consecutive frames.
+constexpr int kSharedSourceThreads = 1024;
+constexpr size_t kSharedSincBytes = size_t(kSharedSincRows) * kSharedSincStride * sizeof(float);
+
+__global__ void __launch_bounds__(kSharedSourceThreads, 1) sharedSourceKernel(BatchView b,
+                                                                               const SharedSource* __restrict__ sources,
+                                                                               const int2* __restrict__ tiles,
+                                                                               int tileCount)
 {
-    const int2 tile = tiles[blockIdx.x];
-    const SharedSource source = sources[tile.x];
-    const cs_voice_span& v = b.voices[source.voice];
-    const int end = min(source.frames, tile.y + kSourceTile);
-    float* out = b.shared + source.offset;
-    const bool stereo = v.channels == 2;
-    #pragma unroll 1
-    for (int i = tile.y + int(threadIdx.x); i < end; i += kSourceThreads) {
-        const float2 x = voiceSource<true>(b.bank, b.sinc, v, v.begin + i, -1.0);
-        if (stereo)
+    extern __shared__ __align__(16) float table[];
+    for (int i = int(threadIdx.x); i < kSharedSincRows * (kTaps / 4); i += kSharedSourceThreads) {
+        const int row = i / (kTaps / 4), quad = i % (kTaps / 4);
+        reinterpret_cast<float4*>(table + row * kSharedSincStride)[quad] =
+            __ldg(reinterpret_cast<const float4*>(b.sinc + size_t(row) * kTaps) + quad);
+    }
+    __syncthreads();
+    const SharedSincRows rows{table};
+    const long long items = (long long)tileCount * kSourceTile;
+    for (long long item = (long long)blockIdx.x * kSharedSourceThreads + threadIdx.x; item < items;
+         item += (long long)gridDim.x * kSharedSourceThreads) {
+        const int2 tile = tiles[item / kSourceTile];
+        const SharedSource source = sources[tile.x];
+        const int i = tile.y + int(item % kSourceTile);
+        if (i >= source.frames)
+            continue;
+        const cs_voice_span& v = b.voices[source.voice];
+        const float2 x = voiceSourceRows<true>(b.bank, rows, v, v.begin + i, -1.0);
+        float* out = b.shared + source.offset;
+        if (v.channels == 2)
             reinterpret_cast<float2*>(out)[i] = x;
         else
             out[i] = x.x;
@@ -1663,14 +1681,6 @@ void launchScan(const BatchView& b, StereoStats* stats, int blocks, cudaStream_t
         scanKernel<<<blocks, kMixThreads, 0, stream>>>(b, stats, blocks);
 }
 
-int launchSharedSources(const BatchView& b, const SharedSource* sources, const int2* tiles, int tileCount,
-                        cudaStream_t stream)
-{
-    if (!tileCount)
-        return 0;
-    sharedSourceKernel<<<tileCount, kSourceThreads, 0, stream>>>(b, sources, tiles);
-    return 1;
-}
 
 void launchPitch(const BatchView& b, const SegmentView& s, cudaStream_t stream)
 {
@@ -1699,6 +1709,24 @@ static void setOncePerDevice(int slot, Set&& set)
         return;
     if (set() == cudaSuccess)
         done[device] |= bit;
+}
+
+int launchSharedSources(const BatchView& b, const SharedSource* sources, const int2* tiles, int tileCount,
+                        cudaStream_t stream)
+{
+    if (!tileCount)
+        return 0;
+    setOncePerDevice(3, [] {
+        return cudaFuncSetAttribute(sharedSourceKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(kSharedSincBytes));
+    });
+    int device = 0, sms = 0;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const long long needed = ((long long)tileCount * kSourceTile + kSharedSourceThreads - 1) / kSharedSourceThreads;
+    const int grid = int(std::max<long long>(1, std::min<long long>(needed, std::max(sms, 1))));
+    sharedSourceKernel<<<grid, kSharedSourceThreads, kSharedSincBytes, stream>>>(b, sources, tiles, tileCount);
+    return 1;
 }
 
 static cudaError_t firstError(std::initializer_list<cudaError_t> statuses)

@@ -543,8 +543,14 @@ SegmentTables planSegments(const HostBatch& batch, size_t budget)
 // (render.cu:63-100 reads nothing else), so a batch renders it once and the mix
 // reads it for each of them.  The audio is unchanged: the source is the same
 // function of the same doubles.  Generators and variable-pitch voices stay inline.
+struct WindowSource;
+
 struct SharedPlan {
     std::vector<SharedSource> sources;
+    // Render windows: the sources sit in the window's pool (offsets are pool
+    // floats), and `claims` are the window sources this batch renders first.
+    bool pooled = false;
+    std::vector<WindowSource*> claims;
     std::vector<SharedRef> refs;        // per voice; empty when nothing is shared
     std::vector<int4> runs;             // (source, 0, frames, first tile) for tile expansion
     size_t tiles = 0, floats = 0;
@@ -577,35 +583,155 @@ long long silentFrom(const cs_voice_span& v)
     }
 }
 
-SharedPlan planSharedSources(const HostBatch& batch, size_t budgetBytes)
+// What a voice's source signal depends on (render.cu:63-100): equal keys give
+// the same source at every elapsed frame.
+struct SourceKey {
+    uint64_t sample;
+    double position, step, slope;
+    int channels, sourceEnd, loopFirst, loopEnd, loopCrossfade;
+    bool operator==(const SourceKey& o) const
+    {
+        return sample == o.sample && position == o.position && step == o.step && slope == o.slope &&
+            channels == o.channels && sourceEnd == o.sourceEnd && loopFirst == o.loopFirst &&
+            loopEnd == o.loopEnd && loopCrossfade == o.loopCrossfade;
+    }
+};
+
+struct SourceKeyHash {
+    size_t operator()(const SourceKey& k) const
+    {
+        uint64_t h = 0x9e3779b97f4a7c15ull;
+        const auto mix = [&h](uint64_t v) { h = (h ^ v) * 0x100000001b3ull; h ^= h >> 29; };
+        uint64_t bits;
+        mix(k.sample);
+        std::memcpy(&bits, &k.position, 8); mix(bits);
+        std::memcpy(&bits, &k.step, 8); mix(bits);
+        std::memcpy(&bits, &k.slope, 8); mix(bits);
+        mix(uint64_t(uint32_t(k.channels)) << 32 | uint32_t(k.sourceEnd));
+        mix(uint64_t(uint32_t(k.loopFirst)) << 32 | uint32_t(k.loopEnd));
+        mix(uint64_t(uint32_t(k.loopCrossfade)));
+        return size_t(h);
+    }
+};
+
+// Whether a voice's source can be shared, its key, and the source frames it
+// needs (to its span's end, or to the frame its source falls silent).
+bool shareable(const cs_voice_span& v)
 {
-    struct Key {
-        uint64_t sample;
-        double position, step, slope;
-        int channels, sourceEnd, loopFirst, loopEnd, loopCrossfade;
-        bool operator==(const Key& o) const
-        {
-            return sample == o.sample && position == o.position && step == o.step && slope == o.slope &&
-                channels == o.channels && sourceEnd == o.sourceEnd && loopFirst == o.loopFirst &&
-                loopEnd == o.loopEnd && loopCrossfade == o.loopCrossfade;
+    return v.filterTrack < 0 && v.generator == CS_GEN_NONE && !v.variablePitch && v.end > v.begin &&
+        v.channels >= 1 && v.channels <= 2;
+}
+
+SourceKey sourceKeyOf(const cs_voice_span& v)
+{
+    return SourceKey{v.sample, v.position, v.step, v.pitchSlope, v.channels, v.sourceEnd, v.loopFirst, v.loopEnd,
+                     v.loopCrossfade};
+}
+
+long long sourceFramesOf(const cs_voice_span& v)
+{
+    long long frames = v.end - v.begin;
+    if (v.loopEnd <= 0 && v.pitchSlope == 0 && v.step > 0)
+        frames = std::min(frames, silentFrom(v));
+    return frames;
+}
+
+// The shared sources of one render window: every source two or more of the
+// window's voices play, at the longest length any of them needs, laid out in one
+// device pool.  The first batch that plays a source renders it there (batches
+// run their kernels in launch order on one stream), and later batches read it.
+struct WindowSource {
+    long long offset = 0;               // floats into the pool
+    int frames = 0, channels = 0, users = 0;
+    bool rendered = false;              // a launched batch renders it
+    bool claimed = false;               // the batch being planned renders it
+};
+
+struct WindowSources {
+    std::unordered_map<SourceKey, WindowSource, SourceKeyHash> map;
+    size_t floats = 0;
+    float* pool = nullptr;
+
+    // Plans the sources of `count` plans; returns the pool floats they need.
+    size_t plan(const cs_plan* plans, size_t count)
+    {
+        map.clear();
+        floats = 0;
+        for (size_t j = 0; j < count; ++j)
+            for (int k = 0; k < plans[j].span_count; ++k) {
+                const cs_voice_span& v = plans[j].spans[k];
+                if (!shareable(v))
+                    continue;
+                WindowSource& w = map[sourceKeyOf(v)];
+                w.frames = int(std::max<long long>(w.frames, sourceFramesOf(v)));
+                w.channels = v.channels;
+                w.users += 1;
+            }
+        for (auto it = map.begin(); it != map.end();) {
+            if (it->second.users < 2 || it->second.frames <= 0) {
+                it = map.erase(it);
+                continue;
+            }
+            it->second.offset = (long long)floats;
+            floats += alignFloats(size_t(it->second.frames) * size_t(it->second.channels));
+            ++it;
         }
-    };
-    struct KeyHash {
-        size_t operator()(const Key& k) const
-        {
-            uint64_t h = 0x9e3779b97f4a7c15ull;
-            const auto mix = [&h](uint64_t v) { h = (h ^ v) * 0x100000001b3ull; h ^= h >> 29; };
-            uint64_t bits;
-            mix(k.sample);
-            std::memcpy(&bits, &k.position, 8); mix(bits);
-            std::memcpy(&bits, &k.step, 8); mix(bits);
-            std::memcpy(&bits, &k.slope, 8); mix(bits);
-            mix(uint64_t(uint32_t(k.channels)) << 32 | uint32_t(k.sourceEnd));
-            mix(uint64_t(uint32_t(k.loopFirst)) << 32 | uint32_t(k.loopEnd));
-            mix(uint64_t(uint32_t(k.loopCrossfade)));
-            return size_t(h);
+        return floats;
+    }
+};
+
+// A batch's share of the window's sources: every voice whose source the window
+// pools reads it there; the sources no earlier batch rendered are this batch's
+// to render, from one of its voices.
+SharedPlan planWindowSources(const HostBatch& batch, WindowSources& window)
+{
+    SharedPlan plan;
+    plan.pooled = true;
+    const size_t count = batch.voices.size();
+    plan.refs.assign(count, SharedRef{-1, 0, 0});
+    bool any = false;
+    for (size_t i = 0; i < count; ++i) {
+        const cs_voice_span& v = batch.voices[i];
+        if (!shareable(v))
+            continue;
+        const auto found = window.map.find(sourceKeyOf(v));
+        if (found == window.map.end())
+            continue;
+        WindowSource& w = found->second;
+        if (!w.rendered && !w.claimed) {
+            w.claimed = true;
+            SharedSource source{};
+            source.offset = w.offset;
+            source.voice = int(i);
+            source.frames = w.frames;
+            plan.runs.push_back(make_int4(int(plan.sources.size()), 0, w.frames, int(plan.tiles)));
+            plan.tiles += size_t(w.frames + kSourceTile - 1) / kSourceTile;
+            plan.sources.push_back(source);
+            plan.claims.push_back(&w);
+            if (resamples(v))
+                plan.sincFloats += (long long)w.frames * w.channels;
         }
-    };
+        plan.refs[i] = SharedRef{w.offset, w.frames, 0};
+        any = true;
+        plan.sharedVoiceFrames += v.end - v.begin;
+        if (resamples(v))
+            plan.sincVoiceFloats += (long long)(v.end - v.begin) * v.channels;
+    }
+    for (WindowSource* w : plan.claims)
+        w->claimed = false;
+    if (!any)
+        plan.refs.clear();
+    if (plan.tiles > size_t(INT32_MAX))
+        throw std::runtime_error("too many shared source tiles in one batch");
+    return plan;
+}
+
+SharedPlan planSharedSources(const HostBatch& batch, size_t budgetBytes, WindowSources* window = nullptr)
+{
+    using Key = SourceKey;
+    using KeyHash = SourceKeyHash;
+    if (window)
+        return planWindowSources(batch, *window);
     struct Entry {
         int voice = -1, frames = 0, users = 0;
         long long total = 0;
@@ -619,14 +745,10 @@ SharedPlan planSharedSources(const HostBatch& batch, size_t budgetBytes)
     std::vector<const Entry*> entryOf(count, nullptr);
     for (size_t i = 0; i < count; ++i) {
         const cs_voice_span& v = batch.voices[i];
-        if (v.filterTrack >= 0 || v.generator != CS_GEN_NONE || v.variablePitch || v.end <= v.begin ||
-            v.channels < 1 || v.channels > 2)
+        if (!shareable(v))
             continue;
-        long long frames = v.end - v.begin;
-        if (v.loopEnd <= 0 && v.pitchSlope == 0 && v.step > 0)
-            frames = std::min(frames, silentFrom(v));
-        const Key key{v.sample, v.position, v.step, v.pitchSlope, v.channels, v.sourceEnd, v.loopFirst, v.loopEnd,
-                      v.loopCrossfade};
+        const long long frames = sourceFramesOf(v);
+        const Key key = sourceKeyOf(v);
         auto found = entries.find(key);
         if (found == entries.end()) {
             entryStore.emplace_back();
@@ -765,9 +887,17 @@ struct cs_renderer {
         void* staging = nullptr;        // page-locked: the lane's batch uploads
         size_t stagingCapacity = 0;
         cudaEvent_t uploaded = nullptr; // the lane's last uploads have been read
+        cudaEvent_t staged = nullptr;   // render windows: the batch's uploads are done
+        cudaEvent_t computed = nullptr; // render windows: the batch's kernels are done
     };
     static constexpr int kLanes = 4;
     Lane lanes[kLanes];
+    // Render windows and serving run every lane's kernels on this one stream, in
+    // batch order, while each lane's uploads and downloads stay on its own stream:
+    // the oldest batch finishes first and its download starts while the next
+    // batches compute (lanes computing side by side all finished late, leaving
+    // the copy engines idle).
+    cudaStream_t compute = nullptr;
     int laneCount = 2;                  // batches in flight at most (cs_renderer_set_lanes)
     float* sinc = nullptr;
     float* bank = nullptr;
@@ -776,6 +906,8 @@ struct cs_renderer {
     bool sharedSources = true;          // render each shared voice source once per batch
     size_t budgetCache = 0;             // derived scratch budget of the current render call (0: stale)
     size_t deferred = 0;                // serving: launches deferred for lack of free memory
+    // Largest staging, download and arena sizes any lane has needed (lanes grow to them).
+    size_t stagingHigh = 0, downloadHigh = 0, arenaHigh = 0;
     size_t oomBudget = 0;               // scratch cap after a lone job's arena did not fit (0: none)
     int failAllocations = 0;            // host-side fault injection: batch arenas to refuse
     struct FailedRequest {              // sizes of the last batch whose arena did not fit
@@ -793,6 +925,11 @@ struct cs_renderer {
     std::unique_ptr<cs::WorkerPool> copier;   // host copies into the staging buffer
     // The job queue and batches in flight behind cs_submit / cs_poll.
     std::unique_ptr<cs::WindowRenderer> service;
+    // The shared-source pool of the render window in progress (null: batches
+    // plan their own shared sources).
+    cs::WindowSources* window = nullptr;
+    void* windowPool = nullptr;
+    size_t windowPoolCapacity = 0;
 
     cs::WorkerPool& copies()
     {
@@ -805,7 +942,11 @@ struct cs_renderer {
 
     // Page-locked host memory that grows on demand (the copy engines read and write
     // it directly).
-    static void* pinned(void*& buffer, size_t& capacity, size_t bytes)
+    // A page-locked buffer of at least `bytes`, grown with a quarter of headroom
+    // and to at least `floor` (the largest size any lane has needed, so that lanes
+    // taking turns at the largest batches do not each reallocate: pinning and
+    // unpinning hundreds of MB stalls the host for tens of milliseconds).
+    static void* pinned(void*& buffer, size_t& capacity, size_t bytes, size_t floor = 0)
     {
         if (bytes <= capacity && buffer)
             return buffer;
@@ -813,7 +954,7 @@ struct cs_renderer {
             cudaFreeHost(buffer);
         buffer = nullptr;
         capacity = 0;
-        const size_t want = std::max<size_t>(bytes + bytes / 4, size_t(1) << 20);
+        const size_t want = std::max<size_t>(std::max(bytes, floor) + std::max(bytes, floor) / 4, size_t(1) << 20);
         if (cudaMallocHost(&buffer, want) != cudaSuccess) {
             cudaGetLastError();
             throw std::runtime_error("cannot allocate pinned host memory");
@@ -907,7 +1048,7 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
                      firstJob, count, t.segments.size(), t.scratchBytes, t.fullScratchBytes);
     r.hostMs[2] += msSince(mark);
     if (r.sharedSources)
-        p->shared = planSharedSources(batch, scratchBudget / 2);
+        p->shared = planSharedSources(batch, scratchBudget / 2, r.window);
     r.hostMs[3] += msSince(mark);
     const SharedPlan& sh = p->shared;
     const size_t jobs = batch.jobs.size();
@@ -956,7 +1097,7 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     const size_t oPacked = section(batch.frames * size_t(channels) * sizeof(short));
     const size_t oSourceTiles = section(t.tileCount * sizeof(int2));
     const size_t oSharedTiles = section(sh.tiles * sizeof(int2));
-    const size_t oShared = section(sh.floats * sizeof(float));
+    const size_t oShared = section(sh.pooled ? 0 : sh.floats * sizeof(float));
     const size_t oScratch = section(t.scratchBytes);
     const size_t oError = section(sizeof(int));
     p->bodyBytes = size_t(batch.bodyWindows) * sizeof(unsigned long long);
@@ -971,8 +1112,16 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
             r.live -= lane.arenaCapacity;
             lane.arena = nullptr;
             lane.arenaCapacity = 0;
-            cudaError_t status = r.failAllocations > 0 ? cudaErrorMemoryAllocation
-                                                       : cudaMalloc(&lane.arena, p->arenaBytes);
+            // Grown to the largest arena any lane has needed, with an eighth of
+            // headroom, falling back to the exact size when that does not fit.
+            r.arenaHigh = std::max(r.arenaHigh, p->arenaBytes);
+            size_t want = r.arenaHigh + r.arenaHigh / 8;
+            cudaError_t status = r.failAllocations > 0 ? cudaErrorMemoryAllocation : cudaMalloc(&lane.arena, want);
+            if (status == cudaErrorMemoryAllocation && r.failAllocations <= 0 && want > p->arenaBytes) {
+                cudaGetLastError();
+                want = p->arenaBytes;
+                status = cudaMalloc(&lane.arena, want);
+            }
             if (r.failAllocations > 0)
                 --r.failAllocations;
             if (status != cudaSuccess) {
@@ -982,7 +1131,7 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
                             uploadEnd};
                 throw CudaError(status, "CUDA batch arena allocation");
             }
-            lane.arenaCapacity = p->arenaBytes;
+            lane.arenaCapacity = want;
             r.live += lane.arenaCapacity;
         }
         p->arena = lane.arena;
@@ -1006,8 +1155,11 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     // lane's previous uploads have been read; other batches use the renderer's.
     if (shared && lane.uploaded)
         check(cudaEventSynchronize(lane.uploaded), "CUDA staging reuse");
-    auto* staging = static_cast<unsigned char*>(shared ? cs_renderer::pinned(lane.staging, lane.stagingCapacity, uploadEnd)
-                                                       : cs_renderer::pinned(r.staging, r.stagingCapacity, uploadEnd));
+    if (shared)
+        r.stagingHigh = std::max(r.stagingHigh, uploadEnd);
+    auto* staging = static_cast<unsigned char*>(
+        shared ? cs_renderer::pinned(lane.staging, lane.stagingCapacity, uploadEnd, r.stagingHigh)
+               : cs_renderer::pinned(r.staging, r.stagingCapacity, uploadEnd));
     std::vector<CopyPiece> pieces;
     const auto stage = [&](size_t offset, const auto& items) {
         if (!items.empty())
@@ -1122,7 +1274,7 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     v.filtered = reinterpret_cast<float*>(base + oScratch);
     v.mix = base + oMix;
     v.error = reinterpret_cast<int*>(base + oError);
-    v.shared = reinterpret_cast<float*>(base + oShared);
+    v.shared = sh.pooled ? r.window->pool : reinterpret_cast<float*>(base + oShared);
     v.sharedRefs = sh.refs.empty() ? nullptr : reinterpret_cast<const SharedRef*>(base + oSharedRefs);
     p->sharedSources = reinterpret_cast<const SharedSource*>(base + oSharedSources);
     p->sharedTiles = reinterpret_cast<const int2*>(base + oSharedTiles);
@@ -1341,7 +1493,8 @@ void enqueueDownload(cs_renderer& r, cs_prepared& p)
     p.downloadResults = 256;
     p.downloadPcm = align256(p.downloadResults + p.resultBytes);
     auto* buffer = static_cast<unsigned char*>(
-        cs_renderer::pinned(lane.download, lane.downloadCapacity, p.downloadPcm + std::max<size_t>(pcmBytes, 1)));
+        cs_renderer::pinned(lane.download, lane.downloadCapacity, p.downloadPcm + std::max<size_t>(pcmBytes, 1),
+                            r.downloadHigh = std::max(r.downloadHigh, p.downloadPcm + std::max<size_t>(pcmBytes, 1))));
     if (!p.copied)
         check(cudaEventCreate(&p.copied), "CUDA download event");
     if (!p.downloading)
@@ -1409,6 +1562,14 @@ public:
         r.oomBudget = 0;
         queue.assign(plans, plans + count);
         next = 0;
+        // One shared-source pool for the whole window (volume groups render
+        // their chunks apart, so they keep per-batch sources).
+        WindowSources window;
+        struct Detach {
+            cs_renderer& r;
+            ~Detach() { r.window = nullptr; }
+        } detach{r};
+        r.window = r.sharedSources && r.groupMinimum <= 0 && poolWindow(window, plans, count) ? &window : nullptr;
         for (;;) {
             launch(true);
             if (flight.empty())
@@ -1417,6 +1578,37 @@ public:
         }
         // The reference's summary line of a render window (jobs, batches, refills).
         std::fprintf(stderr, "SCHEDULE\tjobs=%zu\trounds=%zu\trefills=%zu\n", queue.size(), rounds, refills);
+    }
+
+    // Plans the window's shared sources and places their pool, within half the
+    // scratch budget; false when nothing is shared or the pool does not fit.
+    bool poolWindow(WindowSources& window, const cs_plan* plans, size_t count)
+    {
+        const size_t floats = window.plan(plans, count);
+        if (!floats)
+            return false;
+        if (!r.scratchLimit && !r.budgetCache)
+            r.budgetCache = defaultScratchBudget();
+        const size_t bytes = floats * sizeof(float);
+        if (bytes > (r.scratchLimit ? r.scratchLimit : r.budgetCache) / 2)
+            return false;
+        if (bytes > r.windowPoolCapacity) {
+            cudaFree(r.windowPool);
+            r.live -= r.windowPoolCapacity;
+            r.windowPool = nullptr;
+            r.windowPoolCapacity = 0;
+            const size_t want = bytes + bytes / 8;
+            if (cudaMalloc(&r.windowPool, want) != cudaSuccess) {
+                cudaGetLastError();
+                r.windowPool = nullptr;
+                return false;
+            }
+            r.windowPoolCapacity = want;
+            r.live += want;
+            r.record();
+        }
+        window.pool = static_cast<float*>(r.windowPool);
+        return true;
     }
 
     // cs_submit: queues plans and launches what the free lanes take; returns the
@@ -1516,7 +1708,12 @@ private:
         while (flight.size() < size_t(std::clamp(r.laneCount, 1, cs_renderer::kLanes))) {
             if (next == queue.size() && !(mayRefill && more(flight.empty())))
                 break;
-            size_t jobs = batchEnd(next, std::min(queue.size(), next + r.batchJobs)) - next;
+            // With nothing in flight, a quarter batch starts the device and the
+            // download sooner while the host stages the rest (volume groups keep
+            // whole batches, so their chunking does not change).
+            const size_t want = flight.empty() && r.groupMinimum <= 0 && queue.size() - next > r.batchJobs
+                ? std::max<size_t>(1, r.batchJobs / 4) : r.batchJobs;
+            size_t jobs = batchEnd(next, std::min(queue.size(), next + want)) - next;
             if (admit && !flight.empty()) {
                 if (!freeKnown) {
                     size_t total = 0;
@@ -1547,7 +1744,14 @@ private:
                 next = renderAlone(next, jobs);
                 continue;
             }
-            run(r, *prepared, nullptr);
+            cs_renderer::Lane& l = r.lanes[prepared->lane];
+            check(cudaEventRecord(l.staged, l.stream), "CUDA event record");
+            check(cudaStreamWaitEvent(r.compute, l.staged, 0), "CUDA stream wait");
+            run(r, *prepared, r.compute);
+            for (WindowSource* w : prepared->shared.claims)
+                w->rendered = true;
+            check(cudaEventRecord(l.computed, r.compute), "CUDA event record");
+            check(cudaStreamWaitEvent(l.stream, l.computed, 0), "CUDA stream wait");
             enqueueDownload(r, *prepared);
             ++rounds;
             flight.push_back({prepared, next});
@@ -2034,8 +2238,11 @@ int cs_renderer_create(int device, int natural, const cs_audio_config* audio, in
         r->name = prop.name;
         int leastPriority = 0, greatestPriority = 0;
         cs::check(cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority), "CUDA stream priorities");
+        cs::check(cudaStreamCreateWithFlags(&r->compute, cudaStreamNonBlocking), "CUDA stream");
         for (auto& lane : r->lanes) {
             cs::check(cudaStreamCreateWithFlags(&lane.stream, cudaStreamNonBlocking), "CUDA stream");
+            cs::check(cudaEventCreateWithFlags(&lane.staged, cudaEventDisableTiming), "CUDA event");
+            cs::check(cudaEventCreateWithFlags(&lane.computed, cudaEventDisableTiming), "CUDA event");
             for (int k = 0; k < cs::kLeadTiers; ++k) {
                 cs::check(cudaStreamCreateWithPriority(&lane.lead[k], cudaStreamNonBlocking, greatestPriority),
                           "CUDA stream");
@@ -2065,8 +2272,10 @@ void cs_renderer_destroy(cs_renderer* r)
     cudaSetDevice(r->device);
     for (auto& lane : r->lanes)
         if (lane.stream) cudaStreamSynchronize(lane.stream);
+    if (r->compute) cudaStreamSynchronize(r->compute);
     cudaFree(r->sinc);
     cudaFree(r->bank);
+    cudaFree(r->windowPool);
     for (auto& lane : r->lanes) {
         for (cudaStream_t lead : lane.lead)
             if (lead) cudaStreamSynchronize(lead);
@@ -2078,7 +2287,10 @@ void cs_renderer_destroy(cs_renderer* r)
         if (lane.download) cudaFreeHost(lane.download);
         if (lane.staging) cudaFreeHost(lane.staging);
         if (lane.uploaded) cudaEventDestroy(lane.uploaded);
+        if (lane.staged) cudaEventDestroy(lane.staged);
+        if (lane.computed) cudaEventDestroy(lane.computed);
     }
+    if (r->compute) cudaStreamDestroy(r->compute);
     for (auto& lane : r->lanes) {
         if (lane.stream) cudaStreamDestroy(lane.stream);
         for (int k = 0; k < cs::kLeadTiers; ++k) {

@@ -122,19 +122,56 @@ __device__ __forceinline__ Weights8 sincWeights8(const float* p)
     return r;
 }
 
-// 48-tap windowed-sinc value at `pos` (render.cu:30-61).  The table is stored
-// phase-major, 48 contiguous weights per phase, so each lane streams its row with
-// 256-bit loads; the tap order of the accumulation is unchanged.
-template <bool VectorTaps = false>
-__device__ __forceinline__ float2 sincAt(const float* __restrict__ bank, const float* __restrict__ sinc,
-                                         const cs_voice_span& v, double pos)
+// Sinc weights from the phase-major table in global memory: taps 8q .. 8q + 7 of
+// a phase's row in one 256-bit load.
+struct GlobalSincRows {
+    const float* __restrict__ sinc;
+    __device__ __forceinline__ Weights8 operator()(int phase, int q) const
+    {
+        return sincWeights8(sinc + size_t(phase) * kTaps + 8 * q);
+    }
+};
+
+// Sinc weights from a half table in shared memory: rows 0 .. kPhases / 2, one
+// per phase, kSharedSincStride floats apart (16-byte aligned rows spread over the
+// banks).  The table is symmetric, sinc[tap][phase] == sinc[47 - tap][2048 - phase]
+// exactly (the two arguments are exact negatives, and the window and sin(x)/x are
+// even), so a phase above 1024 reads row 2048 - phase backwards.
+constexpr int kSharedSincStride = 52;
+constexpr int kSharedSincRows = kPhases / 2 + 1;
+
+struct SharedSincRows {
+    const float* table;
+    __device__ __forceinline__ Weights8 operator()(int phase, int q) const
+    {
+        Weights8 r;
+        if (phase <= kPhases / 2) {
+            const float4* row = reinterpret_cast<const float4*>(table + phase * kSharedSincStride + 8 * q);
+            const float4 a = row[0], b = row[1];
+            r.w[0] = a.x; r.w[1] = a.y; r.w[2] = a.z; r.w[3] = a.w;
+            r.w[4] = b.x; r.w[5] = b.y; r.w[6] = b.z; r.w[7] = b.w;
+        } else {
+            // Taps 8q .. 8q + 7 are columns 47 - 8q down to 40 - 8q.
+            const float* row = table + (kPhases - phase) * kSharedSincStride;
+            const float4 a = *reinterpret_cast<const float4*>(row + 44 - 8 * q);
+            const float4 b = *reinterpret_cast<const float4*>(row + 40 - 8 * q);
+            r.w[0] = a.w; r.w[1] = a.z; r.w[2] = a.y; r.w[3] = a.x;
+            r.w[4] = b.w; r.w[5] = b.z; r.w[6] = b.y; r.w[7] = b.x;
+        }
+        return r;
+    }
+};
+
+// 48-tap windowed-sinc value at `pos` (render.cu:30-61), the weights of a phase
+// eight at a time from `rows`; the tap order of the accumulation is unchanged.
+template <bool VectorTaps, class Rows>
+__device__ __forceinline__ float2 sincAtRows(const float* __restrict__ bank, const Rows& rows,
+                                             const cs_voice_span& v, double pos)
 {
     const int center = __double2int_rd(pos);
     if (pos == double(center))
         return sourceFrame(bank, v, center);
     const int phase = __double2int_rn((pos - double(center)) * kPhases);
-    const float4* row = reinterpret_cast<const float4*>(sinc + size_t(phase) * kTaps);
-    const float* row1 = sinc + size_t(phase) * kTaps;
     float x = 0.f, y = 0.f;
     if (center >= 23 && center < v.sourceEnd - 24) {
         const float* s = bank + v.sample + uint64_t(center - 23) * uint64_t(v.channels);
@@ -150,7 +187,7 @@ __device__ __forceinline__ float2 sincAt(const float* __restrict__ bank, const f
             float4 lo = __ldg(s4);
             #pragma unroll
             for (int q = 0; q < kTaps / 8; ++q) {
-                const Weights8 w = sincWeights8(row1 + 8 * q);
+                const Weights8 w = rows(phase, q);
                 const float4 mid = __ldg(s4 + 2 * q + 1), hi = __ldg(s4 + 2 * q + 2);
                 const float f[12] = {lo.x, lo.y, lo.z, lo.w, mid.x, mid.y, mid.z, mid.w, hi.x, hi.y, hi.z, hi.w};
                 float g[10];
@@ -166,7 +203,7 @@ __device__ __forceinline__ float2 sincAt(const float* __restrict__ bank, const f
         } else if (v.channels == 1) {
             #pragma unroll
             for (int q = 0; q < kTaps / 8; ++q) {
-                const Weights8 w = sincWeights8(row1 + 8 * q);
+                const Weights8 w = rows(phase, q);
                 #pragma unroll
                 for (int k = 0; k < 8; ++k)
                     x = fmaf(w.w[k], __ldg(s + 8 * q + k), x);
@@ -176,7 +213,7 @@ __device__ __forceinline__ float2 sincAt(const float* __restrict__ bank, const f
             const float2* s2 = reinterpret_cast<const float2*>(s);
             #pragma unroll
             for (int q = 0; q < kTaps / 8; ++q) {
-                const Weights8 w = sincWeights8(row1 + 8 * q);
+                const Weights8 w = rows(phase, q);
                 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
                     const float2 pk = __ldg(s2 + 8 * q + k);
@@ -187,30 +224,35 @@ __device__ __forceinline__ float2 sincAt(const float* __restrict__ bank, const f
         } else {
             // A stereo sample that starts at an odd float offset (after an odd-length
             // mono sample in the bank) cannot use 8-byte loads.
-            #pragma unroll 4
-            for (int q = 0; q < kTaps / 4; ++q) {
-                const float4 w = __ldg(row + q);
-                const float ws[4] = {w.x, w.y, w.z, w.w};
+            #pragma unroll 2
+            for (int q = 0; q < kTaps / 8; ++q) {
+                const Weights8 w = rows(phase, q);
                 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    x = fmaf(ws[k], __ldg(s + 2 * (4 * q + k)), x);
-                    y = fmaf(ws[k], __ldg(s + 2 * (4 * q + k) + 1), y);
+                for (int k = 0; k < 8; ++k) {
+                    x = fmaf(w.w[k], __ldg(s + 2 * (8 * q + k)), x);
+                    y = fmaf(w.w[k], __ldg(s + 2 * (8 * q + k) + 1), y);
                 }
             }
         }
     } else {
-        for (int q = 0; q < kTaps / 4; ++q) {
-            const float4 w = __ldg(row + q);
-            const float ws[4] = {w.x, w.y, w.z, w.w};
+        for (int q = 0; q < kTaps / 8; ++q) {
+            const Weights8 w = rows(phase, q);
             #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const float2 s = sourceFrame(bank, v, center - 23 + 4 * q + k);
-                x = fmaf(ws[k], s.x, x);
-                y = fmaf(ws[k], s.y, y);
+            for (int k = 0; k < 8; ++k) {
+                const float2 s = sourceFrame(bank, v, center - 23 + 8 * q + k);
+                x = fmaf(w.w[k], s.x, x);
+                y = fmaf(w.w[k], s.y, y);
             }
         }
     }
     return make_float2(x, y);
+}
+
+template <bool VectorTaps = false>
+__device__ __forceinline__ float2 sincAt(const float* __restrict__ bank, const float* __restrict__ sinc,
+                                         const cs_voice_span& v, double pos)
+{
+    return sincAtRows<VectorTaps>(bank, GlobalSincRows{sinc}, v, pos);
 }
 
 // fmod(x, period), which is exact.  For 0 <= x < 2^32 and a positive period it is
@@ -229,9 +271,9 @@ __device__ __forceinline__ double loopRemainder(double x, int period)
 // Source value of a voice at output `frame` (render.cu:63-100): position from the
 // span's start (or a precomputed variable-pitch phase), generators, loop wrap and
 // loop crossfade.
-template <bool VectorTaps = false>
-__device__ __forceinline__ float2 voiceSource(const float* __restrict__ bank, const float* __restrict__ sinc,
-                                              const cs_voice_span& v, int frame, double pos)
+template <bool VectorTaps, class Rows>
+__device__ __forceinline__ float2 voiceSourceRows(const float* __restrict__ bank, const Rows& rows,
+                                                  const cs_voice_span& v, int frame, double pos)
 {
     if (pos < 0) {
         const int elapsed = frame - v.begin;
@@ -258,16 +300,23 @@ __device__ __forceinline__ float2 voiceSource(const float* __restrict__ bank, co
         pos = v.loopFirst + loopRemainder(pos - v.loopFirst, period);
     if (pos >= v.sourceEnd)
         return make_float2(0.f, 0.f);
-    float2 sample = sincAt<VectorTaps>(bank, sinc, v, pos);
+    float2 sample = sincAtRows<VectorTaps>(bank, rows, v, pos);
     const int fadeStart = v.loopEnd - v.loopCrossfade;
     if (v.loopEnd > 0 && v.loopCrossfade > 0 && pos >= fadeStart) {
-        const float2 entry = sincAt<VectorTaps>(bank, sinc, v, pos - period);
+        const float2 entry = sincAtRows<VectorTaps>(bank, rows, v, pos - period);
         const float phase = float((pos - fadeStart) / v.loopCrossfade);
         const float blend = .5f - .5f * cosf(3.14159265358979323846f * phase);
         sample.x = fmaf(blend, entry.x - sample.x, sample.x);
         sample.y = fmaf(blend, entry.y - sample.y, sample.y);
     }
     return sample;
+}
+
+template <bool VectorTaps = false>
+__device__ __forceinline__ float2 voiceSource(const float* __restrict__ bank, const float* __restrict__ sinc,
+                                              const cs_voice_span& v, int frame, double pos)
+{
+    return voiceSourceRows<VectorTaps>(bank, GlobalSincRows{sinc}, v, frame, pos);
 }
 
 __device__ __forceinline__ short toPcm16(float value)

@@ -134,3 +134,33 @@ def test_generators_match_reference(tmp_path, ref_session):
         # Within the contract; not bit for bit (up to 6e-8 FS: the generator voices'
         # arithmetic contracts differently from the reference's in places).
         check_against_reference(plans, bank, mix, pcm, results, exact=False)
+
+
+def test_render_window_shares_sources_across_batches(uneven_jobs, ref_session):
+    """render_window pools the window's shared sources: the first batch that plays
+    a source renders it and later batches read it.  Cut into batches of 8 jobs
+    over four lanes, the first 64 uneven jobs must publish exactly the PCM and
+    results of one plain batch (every voice resampled inline)."""
+    from claysampler_b200.renderer import Renderer
+    plans = [ref_session.plan(j.sfz, j.midi) for j in uneven_jobs]
+    bank = ref_session.bank()
+    _, plain_pcm, plain_results, _ = render(plans, bank, shared=False)
+    renderer = Renderer(natural=True, batch_jobs=8)
+    renderer.set_lanes(4)
+    renderer.upload_samples(bank)
+    jobs = {}
+
+    def publish(batch, first):
+        for k, r in enumerate(batch.results):
+            start = int(r["offset"])
+            jobs[first + k] = (batch.pcm[start:start + int(r["dataFrames"])].copy(), r.copy())
+
+    renderer.render_window(plans, publish)
+    renderer.close()
+    assert sorted(jobs) == list(range(len(plans)))
+    for j, result in enumerate(plain_results):
+        first = int(result["offset"])
+        expected = plain_pcm[first:first + int(result["dataFrames"])]
+        assert np.array_equal(jobs[j][0], expected), j
+        for field in ("status", "frames", "dataFrames", "fade", "peak", "first", "last"):
+            assert jobs[j][1][field] == result[field], (j, field)

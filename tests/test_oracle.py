@@ -22,6 +22,18 @@ def test_sinc_table_matches_reference():
     assert np.array_equal(mine.view(np.uint32), reference.sinc_table().reshape(-1).view(np.uint32))
 
 
+def test_sinc_table_is_symmetric():
+    """sinc[tap][phase] == sinc[47 - tap][2048 - phase] bit for bit: the shared-source
+    kernel keeps only phases 0-1024 in shared memory and reads a phase above 1024
+    as row 2048 - phase backwards."""
+    from oracle import oracle
+    table = np.zeros(48 * 2049, np.float32)
+    oracle.lib().oracle_sinc_table(table.ctypes.data)
+    table = table.reshape(48, 2049)
+    mirrored = table[::-1, ::-1]
+    assert np.array_equal(table.view(np.uint32), mirrored.view(np.uint32))
+
+
 @pytest.mark.parametrize("tail", ["natural", "orig"])
 @pytest.mark.parametrize("fixture", ["plain_small", "batch_mini"])
 def test_restated_render_matches_reference_bit_for_bit(request, ref_session, fixture, tail):
