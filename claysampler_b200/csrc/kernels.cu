@@ -943,6 +943,7 @@ __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(Ba
     __shared__ MixTile tiles[kTilesPerBlock];
     __shared__ TileTrack tracks[kTilesPerBlock][3];     // CC7, CC11, pan
     __shared__ int mixedTiles;          // bit k: tile k is not all staged stereo filtered voices
+    __shared__ int generalTiles;        // bit k: tile k is not all staged kind 5 / 6 voices
     const int block = s.blocks[blockIdx.x];
     const int jobIndex = b.blockJob[block];
     const JobInfo job = b.jobs[jobIndex];
@@ -955,7 +956,7 @@ __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(Ba
         tracks[k][track] = tileTrackOf(b.points, job.tracks[track], job.tracks[track + 1], first, last);
     }
     if (threadIdx.x == 0)
-        mixedTiles = 0;
+        mixedTiles = generalTiles = 0;
     __syncthreads();
     {
         const int k = int(threadIdx.x) / kMixStaged, i = int(threadIdx.x) % kMixStaged;
@@ -963,8 +964,10 @@ __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(Ba
         const MixTile tile = tileIndex < jobTiles ? b.tiles[job.tileFirst + tileIndex] : MixTile{0, 0};
         if (i == 0) {
             tiles[k] = tile;
-            if (tile.count > kMixStaged)
+            if (tile.count > kMixStaged) {
                 atomicOr(&mixedTiles, 1 << k);
+                atomicOr(&generalTiles, 1 << k);
+            }
         }
         if (i < tile.count && tile.count <= kMixStaged) {
             MixVoice m = mixVoiceOf(b, s, __ldg(b.indices + tile.first + i));
@@ -984,12 +987,69 @@ __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(Ba
                     stageEnvelope(m, v, max(first, m.begin), min(last, m.end - 1));
                 }
             }
+            if (m.kind < 5)
+                atomicOr(&generalTiles, 1 << k);
             staged[k][i] = m;
         }
     }
     __syncthreads();
     double power = 0;
     float peak = 0;
+    if (Inline == 2 && generalTiles == 0) {
+        // Every voice of the block is an unmodulated shared-source voice under a
+        // fixed pan: each thread takes four consecutive frames of one tile and
+        // reads each voice's fields once for them (the voices still reach every
+        // frame in span order).
+        const int k = int(threadIdx.x) / (kTileFrames / 4);
+        const int first = local * kBlockFrames + k * kTileFrames + (int(threadIdx.x) % (kTileFrames / 4)) * 4;
+        const MixTile tile = tiles[k];
+        float left[4] = {0.f, 0.f, 0.f, 0.f}, right[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int i = 0; i < tile.count; ++i) {
+            const MixVoice& m = staged[k][i];
+            if (first + 3 < m.begin || first >= m.end)
+                continue;
+            #pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int frame = first + j;
+                if (frame < m.begin || frame >= m.end)
+                    continue;
+                const float level = envelopeOf(m, b.voices, frame);
+                if (level > 0) {
+                    float2 source = make_float2(0.f, 0.f);
+                    if (frame < m.sharedEnd) {
+                        if (m.kind == 5) {
+                            const float x = __ldg(b.shared + (m.offset + frame));
+                            source = make_float2(x, x);
+                        } else {
+                            source = __ldg(reinterpret_cast<const float2*>(b.shared + (m.offset + 2ll * frame)));
+                        }
+                    }
+                    // As voiceOutputFrom: each product rounded before the sum.
+                    left[j] += __fmul_rn(source.x * m.gainLeft, level);
+                    right[j] += __fmul_rn(source.y * m.gainRight, level);
+                }
+            }
+        }
+        #pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int frame = first + j;
+            if (frame >= job.frames || frame < s.first || frame >= s.end)
+                continue;
+            const float amplitude = tileTrackAt(tracks[k][0], b.points, frame) * tileTrackAt(tracks[k][1], b.points, frame);
+            const float x = fmaf(left[j], amplitude, 0.f), y = fmaf(right[j], amplitude, 0.f);
+            if (Natural) {
+                static_cast<float2*>(b.mix)[job.offset + frame] = make_float2(x, y);
+                if (!isfinite(x) || !isfinite(y)) {
+                    peak = __int_as_float(0x7f800000);
+                } else {
+                    peak = fmaxf(peak, fmaxf(fabsf(x), fabsf(y)));
+                    power += double(__fmul_rn(x, x)) + double(__fmul_rn(y, y));
+                }
+            } else {
+                static_cast<short2*>(b.mix)[job.offset + frame] = make_short2(toPcm16(x), toPcm16(y));
+            }
+        }
+    } else
     for (int k = 0; k < kTilesPerBlock; ++k) {
         const int frame = local * kBlockFrames + k * kTileFrames + int(threadIdx.x);
         if (frame >= job.frames || frame < s.first || frame >= s.end)
