@@ -560,16 +560,19 @@ def run_b200(args):
         box["audio"] += float(batch.results["frames"].sum()) / RATE
         box["checksum"] += int(batch.pcm[::4096].astype(np.int64).sum())
 
-    e2e_times = []
+    e2e_times, pass_phases = [], []
     for i in range(args.warmup + args.steps):
         barrier()
         torch.cuda.synchronize()
         box.update(pcm=0, audio=0.0, checksum=0)
+        before = e2e_renderer.host_ms()
         start = time.perf_counter()
         e2e_renderer.render_window(plan_set, publish, copy=False)
         elapsed = time.perf_counter() - start
+        after = e2e_renderer.host_ms()
         if i >= args.warmup:
             e2e_times.append(elapsed)
+            pass_phases.append({k: round(after[k] - before[k], 2) for k in after})
     e2e_s = sum(e2e_times) / len(e2e_times)
     host_ms = {k: v / (args.warmup + args.steps) for k, v in e2e_renderer.host_ms().items()}
 
@@ -628,7 +631,9 @@ def run_b200(args):
                "e2e": {"value": total_e2e_audio / max_e2e, "unit": "audio-s/s", "h2d_bytes_per_step": int(h2d),
                        "d2h_bytes_per_step": int(box.get("pcm", 0)), "ms_per_step": max_e2e * 1e3,
                        "batch_jobs": e2e_batch, "autotune": tuned, "host_staging_ms_per_step": host_ms,
-                       "pass_ms": [round(t * 1e3, 2) for t in e2e_times]},
+                       "pass_ms": [round(t * 1e3, 2) for t in e2e_times],
+                       "median_ms": round(statistics.median(e2e_times) * 1e3, 2),
+                       "slowest_pass_host_ms": pass_phases[int(np.argmax(e2e_times))] if pass_phases else None},
                "gpu_launches": launches, "clocks": clocks.summary()}
         if world == 1:
             try:

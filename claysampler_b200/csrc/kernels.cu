@@ -1475,7 +1475,9 @@ __global__ void layoutKernel(BatchView b, FinishView f, int natural)
     }
 }
 
-__device__ __forceinline__ short fadeSample(short value, int index, int count)
+// Out of line: only the last frames of a job fade, and the FP64 cosine would
+// otherwise hold registers through the whole finishing loop.
+__device__ __noinline__ short fadeSample(short value, int index, int count)
 {
     constexpr double pi = 3.14159265358979323846;
     const double gain = count == 1 ? 0 : .5 * (1 + cos(pi * index / (count - 1)));
@@ -1488,8 +1490,8 @@ __device__ __forceinline__ short fadeSample(short value, int index, int count)
 // sums are integers, so the warp partials and atomics give the reference's
 // totals in any order.  A warp per 1024-frame block (eight per CTA), each lane
 // every 32nd frame; the reductions are warp shuffles, so no CTA barrier is needed.
-template <int Channels>
-__global__ void __launch_bounds__(kFinalizeWarps * 32) finalizeKernel(BatchView b, FinishView f, const short* input,
+template <int Channels, bool Assess>
+__global__ void __launch_bounds__(kFinalizeWarps * 32, Assess ? 4 : 6) finalizeKernel(BatchView b, FinishView f, const short* input,
                                                                       int quality)
 {
     const int block = int(blockIdx.x) * kFinalizeWarps + int(threadIdx.x >> 5);
@@ -1508,7 +1510,7 @@ __global__ void __launch_bounds__(kFinalizeWarps * 32) finalizeKernel(BatchView 
     // Body windows this block touches: [windowA, windowB]; frames before `split`
     // belong to windowA.
     int bodyEnd = 0, windowA = 0, windowB = 0, split = 0, bodyFirst = 0;
-    if (f.bodyPower && result.status == CS_TAIL_OK) {
+    if (Assess && f.bodyPower && result.status == CS_TAIL_OK) {
         const AssessJob a = f.assess[jobIndex];
         bodyEnd = min(a.bodyFrames, end);
         bodyFirst = a.bodyFirst;
@@ -1547,6 +1549,7 @@ __global__ void __launch_bounds__(kFinalizeWarps * 32) finalizeKernel(BatchView 
                 packed[frame * Channels + c] = value;
                 const int magnitude = abs(int(value));
                 framePeak = max(framePeak, magnitude);
+                if (Assess)
                 clipped += magnitude >= 32767;
                 mono += Channels == 1 ? 2 * int(value) : int(value);
             }
@@ -1555,7 +1558,7 @@ __global__ void __launch_bounds__(kFinalizeWarps * 32) finalizeKernel(BatchView 
                 audibleFirst = min(audibleFirst, frame);
                 audibleLast = frame;
             }
-            if (frame < bodyEnd) {
+            if (Assess && frame < bodyEnd) {
                 const unsigned long long power = (unsigned long long)((long long)mono * mono);
                 if (!paired)
                     atomicAdd(f.bodyPower + bodyFirst + f.body.windowOf(frame), power);
@@ -1569,8 +1572,9 @@ __global__ void __launch_bounds__(kFinalizeWarps * 32) finalizeKernel(BatchView 
     peak = warpAll(peak, MaxOp{});
     audibleFirst = warpAll(audibleFirst, MinOp{});
     audibleLast = warpAll(audibleLast, MaxOp{});
-    clipped = warpAll(clipped, SumOp{});
-    if (first < bodyEnd && paired) {
+    if (Assess)
+        clipped = warpAll(clipped, SumOp{});
+    if (Assess && first < bodyEnd && paired) {
         powerA = warpAll(powerA, SumOp{});
         powerB = warpAll(powerB, SumOp{});
         if (lane == 0) {
@@ -1580,7 +1584,7 @@ __global__ void __launch_bounds__(kFinalizeWarps * 32) finalizeKernel(BatchView 
         }
     }
     if (lane == 0) {
-        if (quality && clipped)
+        if (Assess && quality && clipped)
             atomicAdd(&result.audio.clipped, clipped);
         if (audibleLast >= 0) {
             atomicMax(&result.peak, peak);
@@ -1898,13 +1902,17 @@ int launchFinish(const BatchView& b, const FinishView& f, bool natural, bool qua
     layoutKernel<<<1, 32, 0, stream>>>(b, f, natural ? 1 : 0);
     ++launches;
     if (f.blockCount) {
-        if (natural)
-            finalizeKernel<1><<<(f.blockCount + kFinalizeWarps - 1) / kFinalizeWarps, kFinalizeWarps * 32, 0, stream>>>(
-                b, f, f.mono, quality ? 1 : 0);
+        const int grid = (f.blockCount + kFinalizeWarps - 1) / kFinalizeWarps, threads = kFinalizeWarps * 32;
+        const short* pcm = natural ? f.mono : static_cast<const short*>(b.mix);
+        const bool assess = quality || f.bodyPower;
+        if (natural && assess)
+            finalizeKernel<1, true><<<grid, threads, 0, stream>>>(b, f, pcm, quality ? 1 : 0);
+        else if (natural)
+            finalizeKernel<1, false><<<grid, threads, 0, stream>>>(b, f, pcm, 0);
+        else if (assess)
+            finalizeKernel<2, true><<<grid, threads, 0, stream>>>(b, f, pcm, quality ? 1 : 0);
         else
-            finalizeKernel<2><<<(f.blockCount + kFinalizeWarps - 1) / kFinalizeWarps, kFinalizeWarps * 32, 0, stream>>>(
-                b, f, static_cast<const short*>(b.mix),
-                                                              quality ? 1 : 0);
+            finalizeKernel<2, false><<<grid, threads, 0, stream>>>(b, f, pcm, 0);
         ++launches;
     }
     return launches;

@@ -636,9 +636,8 @@ long long sourceFramesOf(const cs_voice_span& v)
     return frames;
 }
 
-// The shared sources of one render window: every source two or more of the
-// window's voices play, at the longest length any of them needs, laid out in one
-// device pool.  The first batch that plays a source renders it there (batches
+// The shared sources of one render window: every source the window's voices
+// play, at the longest length any of them needs, laid out in one device pool.  The first batch that plays a source renders it there (batches
 // run their kernels in launch order on one stream), and later batches read it.
 struct WindowSource {
     long long offset = 0;               // floats into the pool
@@ -668,7 +667,7 @@ struct WindowSources {
                 w.users += 1;
             }
         for (auto it = map.begin(); it != map.end();) {
-            if (it->second.users < 2 || it->second.frames <= 0) {
+            if (it->second.frames <= 0) {
                 it = map.erase(it);
                 continue;
             }
@@ -762,13 +761,13 @@ SharedPlan planSharedSources(const HostBatch& batch, size_t budgetBytes, WindowS
         e.total += frames;
         entryOf[i] = &e;
     }
-    // Sources played by more than one voice, the most voice frames saved first,
-    // within the budget.
-    // Candidates in order of first use (deterministic), then by the voice frames
-    // they save.
+    // Every source, the most voice frames saved first, within the budget; in
+    // order of first use among equals (deterministic).  A source only one voice
+    // plays saves no resampling, but once every unfiltered voice reads a shared
+    // source the mix runs without its inline resampler.
     std::vector<Entry*> chosen;
     for (Entry& e : entryStore)
-        if (e.users > 1 && e.frames > 0)
+        if (e.frames > 0)
             chosen.push_back(&e);
     std::stable_sort(chosen.begin(), chosen.end(), [](const Entry* a, const Entry* b) {
         return a->total - a->frames > b->total - b->frames;
