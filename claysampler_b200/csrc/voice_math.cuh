@@ -271,17 +271,21 @@ __device__ __forceinline__ double loopRemainder(double x, int period)
 // Source value of a voice at output `frame` (render.cu:63-100): position from the
 // span's start (or a precomputed variable-pitch phase), generators, loop wrap and
 // loop crossfade.
+// A voice's source position `elapsed` frames into its span (render.cu:65-70).
+__device__ __forceinline__ double sourcePosition(const cs_voice_span& v, int elapsed)
+{
+    double distance = elapsed;
+    if (v.pitchSlope != 0)
+        distance = expm1(v.pitchSlope * elapsed) / expm1(v.pitchSlope);
+    return v.position + distance * v.step;
+}
+
 template <bool VectorTaps, class Rows>
 __device__ __forceinline__ float2 voiceSourceRows(const float* __restrict__ bank, const Rows& rows,
                                                   const cs_voice_span& v, int frame, double pos)
 {
-    if (pos < 0) {
-        const int elapsed = frame - v.begin;
-        double distance = elapsed;
-        if (v.pitchSlope != 0)
-            distance = expm1(v.pitchSlope * elapsed) / expm1(v.pitchSlope);
-        pos = v.position + distance * v.step;
-    }
+    if (pos < 0)
+        pos = sourcePosition(v, frame - v.begin);
     if (v.generator != CS_GEN_NONE) {
         if (v.generator == CS_GEN_NOISE) {
             unsigned bits = v.noiseSeed + unsigned(frame - v.noiseStart);
