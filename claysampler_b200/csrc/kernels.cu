@@ -757,24 +757,34 @@ __global__ void __launch_bounds__(kSharedSourceThreads, 1) sharedSourceKernel(Ba
 
 constexpr int kMixThreads = 256;
 
-template <class T, class Op>
-__device__ __forceinline__ T blockReduce(T value, T identity, Op op, T* scratch)
+
+// The block's power (sum) and peak (maximum) at once, one barrier; valid in
+// thread 0.  `sums` and `peaks` hold a slot per warp and serve no other use.
+__device__ __forceinline__ void blockStats(double& power, float& peak, double* sums, float* peaks)
 {
     #pragma unroll
-    for (int d = 16; d; d >>= 1)
-        value = op(value, __shfl_down_sync(0xffffffffu, value, d));
+    for (int d = 16; d; d >>= 1) {
+        power += __shfl_down_sync(0xffffffffu, power, d);
+        const float other = __shfl_down_sync(0xffffffffu, peak, d);
+        peak = other > peak ? other : peak;
+    }
     const int warp = int(threadIdx.x >> 5), lane = int(threadIdx.x & 31);
-    __syncthreads();
-    if (!lane)
-        scratch[warp] = value;
+    if (!lane) {
+        sums[warp] = power;
+        peaks[warp] = peak;
+    }
     __syncthreads();
     if (warp == 0) {
-        value = lane < int(blockDim.x >> 5) ? scratch[lane] : identity;
+        const bool held = lane < int(blockDim.x >> 5);
+        power = held ? sums[lane] : 0.0;
+        peak = held ? peaks[lane] : 0.f;
         #pragma unroll
-        for (int d = 16; d; d >>= 1)
-            value = op(value, __shfl_down_sync(0xffffffffu, value, d));
+        for (int d = 16; d; d >>= 1) {
+            power += __shfl_down_sync(0xffffffffu, power, d);
+            const float other = __shfl_down_sync(0xffffffffu, peak, d);
+            peak = other > peak ? other : peak;
+        }
     }
-    return value;                       // valid in thread 0
 }
 
 struct SumOp { template <class T> __device__ T operator()(T a, T b) const { return a + b; } };
@@ -942,8 +952,9 @@ __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(Ba
     __shared__ MixVoice staged[kTilesPerBlock][kMixStaged];
     __shared__ MixTile tiles[kTilesPerBlock];
     __shared__ TileTrack tracks[kTilesPerBlock][3];     // CC7, CC11, pan
-    __shared__ int mixedTiles;          // bit k: tile k is not all staged stereo filtered voices
-    __shared__ int generalTiles;        // bit k: tile k is not all staged kind 5 / 6 voices
+    // Per warp: bit k of mixed / general marks tile k as not all staged stereo
+    // filtered voices / not all staged kind 5 / 6 voices.
+    __shared__ unsigned warpFlags[kMixThreads / 32][2];
     const int block = s.blocks[blockIdx.x];
     const int jobIndex = b.blockJob[block];
     const JobInfo job = b.jobs[jobIndex];
@@ -955,27 +966,25 @@ __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(Ba
         const int last = min(first + kTileFrames, max(job.frames, first + 1)) - 1;
         tracks[k][track] = tileTrackOf(b.points, job.tracks[track], job.tracks[track + 1], first, last);
     }
-    if (threadIdx.x == 0)
-        mixedTiles = generalTiles = 0;
-    __syncthreads();
     {
         const int k = int(threadIdx.x) / kMixStaged, i = int(threadIdx.x) % kMixStaged;
         const int tileIndex = local * kTilesPerBlock + k;
         const MixTile tile = tileIndex < jobTiles ? b.tiles[job.tileFirst + tileIndex] : MixTile{0, 0};
+        unsigned mixed = 0, general = 0;
         if (i == 0) {
             tiles[k] = tile;
-            if (tile.count > kMixStaged) {
-                atomicOr(&mixedTiles, 1 << k);
-                atomicOr(&generalTiles, 1 << k);
-            }
+            if (tile.count > kMixStaged)
+                mixed = general = 1u << k;
         }
         if (i < tile.count && tile.count <= kMixStaged) {
             MixVoice m = mixVoiceOf(b, s, __ldg(b.indices + tile.first + i));
             if (m.kind != 1)
-                atomicOr(&mixedTiles, 1 << k);
-            const TileTrack pan = tracks[k][2];
+                mixed |= 1u << k;
             const int first = local * kBlockFrames + k * kTileFrames;
             if (m.kind >= 3) {
+                // The tile's pan track, as the track staging above finds it.
+                const TileTrack pan = tileTrackOf(b.points, job.tracks[2], job.tracks[3], first,
+                                                  min(first + kTileFrames, max(job.frames, first + 1)) - 1);
                 const cs_voice_span& v = b.voices[m.index];
                 if (v.modulationCount == 0 && !v.stereoMatrix && tileTrackFixed(pan, first)) {
                     // voiceOutputFrom with no bindings: the pan offset is the track's.
@@ -988,11 +997,23 @@ __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(Ba
                 }
             }
             if (m.kind < 5)
-                atomicOr(&generalTiles, 1 << k);
+                general |= 1u << k;
             staged[k][i] = m;
+        }
+        mixed = __reduce_or_sync(0xffffffffu, mixed);
+        general = __reduce_or_sync(0xffffffffu, general);
+        if ((threadIdx.x & 31) == 0) {
+            warpFlags[threadIdx.x >> 5][0] = mixed;
+            warpFlags[threadIdx.x >> 5][1] = general;
         }
     }
     __syncthreads();
+    unsigned mixedTiles = 0, generalTiles = 0;
+    #pragma unroll
+    for (int w = 0; w < kMixThreads / 32; ++w) {
+        mixedTiles |= warpFlags[w][0];
+        generalTiles |= warpFlags[w][1];
+    }
     double power = 0;
     float peak = 0;
     if (Inline == 2 && generalTiles == 0) {
@@ -1170,8 +1191,7 @@ __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(Ba
         }
     }
     if (Natural) {
-        power = blockReduce(power, 0.0, SumOp{}, reduceD);
-        peak = blockReduce(peak, 0.f, MaxOp{}, reduceF);
+        blockStats(power, peak, reduceD, reduceF);
         if (threadIdx.x == 0)
             stats[block] = {power, peak};
     }
@@ -1201,8 +1221,7 @@ __global__ void __launch_bounds__(kMixThreads) scanKernel(BatchView b, StereoSta
             power += double(__fmul_rn(v.x, v.x)) + double(__fmul_rn(v.y, v.y));
         }
     }
-    power = blockReduce(power, 0.0, SumOp{}, reduceD);
-    peak = blockReduce(peak, 0.f, MaxOp{}, reduceF);
+    blockStats(power, peak, reduceD, reduceF);
     if (threadIdx.x == 0)
         stats[block] = {power, peak};
 }
