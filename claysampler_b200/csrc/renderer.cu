@@ -2,7 +2,11 @@
 //
 // A batch of plans becomes one device arena holding the spans, control points,
 // modulation bindings, per-job records, mix tiles, the float mix and the finishing
-// buffers.  Voice chains that need filter or pitch storage write it to a scratch
+// buffers.  Render windows (cs_render_window, cs_submit / cs_poll) keep up to four
+// batches in flight, each on a stream lane with its own arena and page-locked
+// staging and download buffers; their kernels run in batch order on one compute
+// stream, and within a render window the shared voice sources are pooled across
+// its batches.  Voice chains that need filter or pitch storage write it to a scratch
 // region; when that storage exceeds the scratch budget the job timeline is cut into
 // 1024-frame-aligned segments and chain state (filter history, coefficient
 // smoothing, pitch phase) carries across them in ChainState, as the reference's
@@ -59,8 +63,9 @@ struct Layout {
 };
 
 // The reference's BatchIndex::append (src/cuda/renderer.cpp:390-460) restated for
-// this renderer's layout: 256-frame tiles with span-ordered voice lists, rebased
-// control and modulation offsets, and voice chains linked by nextFilteredSpan.
+// this renderer's layout: rebased control and modulation offsets, voice chains
+// linked by nextFilteredSpan, and per job the inputs from which tileIndexKernel
+// builds the 256-frame tiles' span-ordered voice lists on the device.
 struct HostBatch {
     std::vector<cs_voice_span> voices;
     // Control points stay in the callers' plans; each plan's points are copied once,
