@@ -549,6 +549,7 @@ def run_b200(args):
     if tuned:
         e2e_renderer.set_lanes(tuned["lanes"])
         e2e_renderer.set_shared_sources(tuned["shared_sources"])
+        e2e_renderer.set_ordered_compute(tuned["ordered_compute"])
     e2e_renderer.upload_samples(bank)
     h2d = sum(p.spans.nbytes + p.points.nbytes + p.modulation.nbytes + p.track_offsets.nbytes for p in plans)
     box = {}

@@ -13,6 +13,9 @@ end-to-end rate without changing a sample is how the work is cut and overlapped:
 * `shared_sources`: whether each distinct resampled source is rendered once per
   batch and read by every voice that plays it, or every voice frame is resampled
   inline.  Which is faster depends on how often sources repeat in a batch.
+* `ordered_compute`: whether every lane's kernels run in batch order on one stream
+  (downloads start early; shared sources pooled per window) or each lane's beside
+  the others (latency-bound kernels such as long filter chains overlap).
 
 The best point depends on the workload's lengths and voice mix, so :func:`tune`
 measures it.  After one discarded warm-up, it renders the workload through
@@ -50,14 +53,16 @@ def signature(plans) -> str:
 
 
 def measure(plans, bank, batch_jobs: int, repeats: int = 2, device: int = 0, lanes: int = 2,
-            shared_sources: bool = True) -> float:
+            shared_sources: bool = True, ordered_compute: bool = True) -> float:
     """Output audio-seconds per second of render_window with GPU batches of
-    `batch_jobs`, `lanes` batches in flight and shared sources on or off."""
+    `batch_jobs`, `lanes` batches in flight, shared sources on or off and the
+    lanes' kernels ordered on one stream or side by side."""
     plans = plans if isinstance(plans, PlanSet) else PlanSet(plans)
     renderer = Renderer(device=device, natural=True, batch_jobs=batch_jobs)
     try:
         renderer.set_lanes(lanes)
         renderer.set_shared_sources(shared_sources)
+        renderer.set_ordered_compute(ordered_compute)
         renderer.upload_samples(bank)
         audio = [0.0]
 
@@ -79,14 +84,15 @@ def measure(plans, bank, batch_jobs: int, repeats: int = 2, device: int = 0, lan
 def tune(plans, bank, candidates=CANDIDATES, repeats: int = 3, device: int = 0,
          cache: Path | None = None, lanes=LANES, shared=SHARED) -> dict:
     """The fastest render_window settings for `plans`: {"batch_jobs", "lanes",
-    "shared_sources", "sweep", "signature"}.  The batch size is swept first with
-    two lanes and shared sources; the lane counts and the source mode are then
-    tried at the two best sizes."""
+    "shared_sources", "ordered_compute", "sweep", "signature"}.  The batch size is
+    swept first with two lanes and shared sources; the lane counts and the source
+    mode are then tried at the two best sizes, and the lanes' kernels side by side
+    at the best point."""
     key = signature(plans)
     store = {}
     if cache is not None and cache.exists():
         store = json.loads(cache.read_text())
-        if key in store and "lanes" in store[key]:
+        if key in store and "ordered_compute" in store[key]:
             return store[key]
     measure(plans, bank, candidates[0], 1, device)        # one-time costs (threads, page-locking) land here
     sweep = {}
@@ -103,9 +109,13 @@ def tune(plans, bank, candidates=CANDIDATES, repeats: int = 3, device: int = 0,
                 name = f"{best_jobs}/{count}/{'shared' if mode else 'plain'}"
                 if name not in sweep:
                     sweep[name] = measure(plans, bank, int(best_jobs), repeats, device, count, mode)
+    # The lanes side by side at the best point so far.
+    best = max(sweep, key=sweep.get).split("/")
+    name = "/".join(best) + "/side"
+    sweep[name] = measure(plans, bank, int(best[0]), repeats, device, int(best[1]), best[2] == "shared", False)
     best = max(sweep, key=sweep.get).split("/")
     result = {"batch_jobs": int(best[0]), "lanes": int(best[1]), "shared_sources": best[2] == "shared",
-              "sweep": sweep, "signature": key}
+              "ordered_compute": len(best) < 4, "sweep": sweep, "signature": key}
     if cache is not None:
         store[key] = result
         cache.parent.mkdir(parents=True, exist_ok=True)

@@ -902,6 +902,10 @@ struct cs_renderer {
     // batches compute (lanes computing side by side all finished late, leaving
     // the copy engines idle).
     cudaStream_t compute = nullptr;
+    // Off: each lane runs its kernels on its own stream beside the others (for
+    // batches whose latency-bound kernels leave the GPU room), and render windows
+    // plan their shared sources per batch (nothing orders the lanes' kernels).
+    bool orderedCompute = true;
     int laneCount = 2;                  // batches in flight at most (cs_renderer_set_lanes)
     float* sinc = nullptr;
     float* bank = nullptr;
@@ -1573,7 +1577,8 @@ public:
             cs_renderer& r;
             ~Detach() { r.window = nullptr; }
         } detach{r};
-        r.window = r.sharedSources && r.groupMinimum <= 0 && poolWindow(window, plans, count) ? &window : nullptr;
+        r.window = r.sharedSources && r.orderedCompute && r.groupMinimum <= 0 && poolWindow(window, plans, count)
+            ? &window : nullptr;
         for (;;) {
             launch(true);
             if (flight.empty())
@@ -1748,14 +1753,18 @@ private:
                 next = renderAlone(next, jobs);
                 continue;
             }
-            cs_renderer::Lane& l = r.lanes[prepared->lane];
-            check(cudaEventRecord(l.staged, l.stream), "CUDA event record");
-            check(cudaStreamWaitEvent(r.compute, l.staged, 0), "CUDA stream wait");
-            run(r, *prepared, r.compute);
-            for (WindowSource* w : prepared->shared.claims)
-                w->rendered = true;
-            check(cudaEventRecord(l.computed, r.compute), "CUDA event record");
-            check(cudaStreamWaitEvent(l.stream, l.computed, 0), "CUDA stream wait");
+            if (r.orderedCompute) {
+                cs_renderer::Lane& l = r.lanes[prepared->lane];
+                check(cudaEventRecord(l.staged, l.stream), "CUDA event record");
+                check(cudaStreamWaitEvent(r.compute, l.staged, 0), "CUDA stream wait");
+                run(r, *prepared, r.compute);
+                for (WindowSource* w : prepared->shared.claims)
+                    w->rendered = true;
+                check(cudaEventRecord(l.computed, r.compute), "CUDA event record");
+                check(cudaStreamWaitEvent(l.stream, l.computed, 0), "CUDA stream wait");
+            } else {
+                run(r, *prepared, nullptr);
+            }
             enqueueDownload(r, *prepared);
             ++rounds;
             flight.push_back({prepared, next});
@@ -2527,6 +2536,17 @@ int cs_renderer_fail_allocations(cs_renderer* r, int count)
         if (!r || count < 0)
             throw std::runtime_error("invalid allocation-failure count");
         r->failAllocations = count;
+    });
+}
+
+int cs_renderer_set_ordered_compute(cs_renderer* r, int ordered)
+{
+    return cs::guardedOn(r, [&] {
+        if (!r)
+            throw std::runtime_error("null renderer");
+        if (r->service && (r->service->pending() || r->service->inFlight()))
+            throw std::runtime_error("submitted jobs are in flight; poll them first");
+        r->orderedCompute = ordered != 0;
     });
 }
 

@@ -59,6 +59,7 @@ def library() -> ctypes.CDLL:
         lib.cs_renderer_host_ms.argtypes = [vp, c.POINTER(c.c_double), i32]
         lib.cs_renderer_set_lanes.argtypes = [vp, i32]
         lib.cs_renderer_fail_allocations.argtypes = [vp, i32]
+        lib.cs_renderer_set_ordered_compute.argtypes = [vp, i32]
         lib.cs_renderer_deferred_launches.argtypes = [vp]
         lib.cs_renderer_deferred_launches.restype = sz
         for name in ("cs_prepared_shared_sources", "cs_prepared_shared_frames"):
@@ -237,6 +238,11 @@ class Renderer:
     def set_lanes(self, lanes: int) -> None:
         """Batches in flight at most (1-4); submit / poll publishes them as they finish."""
         _check(library().cs_renderer_set_lanes(self.handle, lanes))
+
+    def set_ordered_compute(self, ordered: bool) -> None:
+        """True (default): every lane's kernels in batch order on one stream, shared
+        sources pooled per render window; False: lanes compute side by side."""
+        _check(library().cs_renderer_set_ordered_compute(self.handle, int(bool(ordered))))
 
     def fail_allocations(self, count: int) -> None:
         """Test hook: the next `count` batch-arena allocations report out of memory

@@ -290,6 +290,14 @@ int cs_renderer_set_lanes(cs_renderer* renderer, int lanes);
  * flight and free the other lanes' arenas, halve the batch, halve a lone job's
  * scratch budget, reject the job; src/cuda/renderer.cpp:947-992).  0 turns it off. */
 int cs_renderer_fail_allocations(cs_renderer* renderer, int count);
+/* 1 (default): render windows and serving run every lane's kernels on one stream
+ * in batch order (the oldest batch finishes first and its download overlaps the
+ * next batches' kernels), and a render window pools its shared voice sources
+ * across its batches.  0: each lane runs its kernels on its own stream beside the
+ * others, which suits batches whose latency-bound kernels (long filter chains)
+ * leave the GPU room, and shared sources are planned per batch.  The audio is the
+ * same either way.  No counterpart in the reference. */
+int cs_renderer_set_ordered_compute(cs_renderer* renderer, int ordered);
 /* Serving: how often a batch launch waited because its estimated footprint
  * exceeded half of the free device memory while other batches were in flight. */
 size_t cs_renderer_deferred_launches(const cs_renderer* renderer);

@@ -27,13 +27,15 @@ def test_tuned_batching_keeps_every_job_identical(ref_session, batch_mini, plain
     assert {"1/2/shared", "2/2/shared", "8/2/shared"} <= set(tuned["sweep"])
     best = tuned["batch_jobs"]
     assert {f"{best}/2/shared", f"{best}/2/plain", f"{best}/4/shared", f"{best}/4/plain"} <= set(tuned["sweep"])
+    assert any(name.endswith("/side") for name in tuned["sweep"]) and isinstance(tuned["ordered_compute"], bool)
     assert all(v > 0 for v in tuned["sweep"].values())
     assert autotune.tune(plans, bank, candidates=(1, 2, 8), cache=cache) == tuned   # cached
 
-    def render(batch_jobs, lanes=2, shared=True):
+    def render(batch_jobs, lanes=2, shared=True, ordered=True):
         renderer = Renderer(natural=True, batch_jobs=batch_jobs)
         renderer.set_lanes(lanes)
         renderer.set_shared_sources(shared)
+        renderer.set_ordered_compute(ordered)
         renderer.upload_samples(bank)
         jobs = {}
 
@@ -47,7 +49,11 @@ def test_tuned_batching_keeps_every_job_identical(ref_session, batch_mini, plain
         return jobs
 
     one = render(1, 1, False)
-    tuned_jobs = render(tuned["batch_jobs"], tuned["lanes"], tuned["shared_sources"])
+    tuned_jobs = render(tuned["batch_jobs"], tuned["lanes"], tuned["shared_sources"], tuned["ordered_compute"])
+    side_jobs = render(2, 4, True, False)
+    assert sorted(side_jobs) == sorted(one)
+    for j in one:
+        np.testing.assert_array_equal(one[j][0], side_jobs[j][0])
     assert sorted(one) == sorted(tuned_jobs) == list(range(len(plans)))
     for j in one:
         np.testing.assert_array_equal(one[j][0], tuned_jobs[j][0])
