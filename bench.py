@@ -105,6 +105,8 @@ def parse():
     p.add_argument("--serve-rate", type=float, default=50.0)
     p.add_argument("--serve-lanes", type=int, default=4, help="batches in flight (cs_renderer_set_lanes)")
     p.add_argument("--serve-batch", type=int, default=32, help="jobs per batch at most")
+    p.add_argument("--serve-bank", choices=("small", "large"), default="small",
+                   help="presets of the small kind, or of the HBM-bank kind (8 presets: about 12 GB of samples)")
     return p.parse_args()
 
 
@@ -658,10 +660,12 @@ def serving_requests(args, rank):
     and sample bank."""
     from claysampler_b200 import workload as wl
     from claysampler_b200.host import Host
-    root = args.workdir / f"serving_s{args.seed + rank}_j{args.serve_jobs}_r{args.serve_rate:g}"
+    large = args.serve_bank == "large"
+    root = args.workdir / f"serving_s{args.seed + rank}_j{args.serve_jobs}_r{args.serve_rate:g}{'_large' if large else ''}"
     marker = root / "ready"
     if not marker.exists():
-        jobs, arrivals = wl.write_serving_jobs(root, seed=args.seed + rank, jobs=args.serve_jobs, rate=args.serve_rate)
+        jobs, arrivals = wl.write_serving_jobs(root, seed=args.seed + rank, jobs=args.serve_jobs, rate=args.serve_rate,
+                                               large=large)
         marker.write_text("\n".join(f"{j.sfz}\t{j.midi}\t{float(t)!r}" for j, t in zip(jobs, arrivals)))
     rows = [line.split("\t") for line in marker.read_text().splitlines()]
     host = Host()
@@ -720,7 +724,9 @@ def run_serve(args):
            "offered_audio_s_per_s": offered, "jobs": len(submitted), "rate_jobs_per_s": args.serve_rate,
            "wall_s": wall, "n_gpus": 1, "dtype": "f32", "data": "synthetic (seeded SFZ/WAV/MIDI)",
            "deferred_launches": renderer.deferred_launches,
-           "config": {"workload": "requests of the small kind over 8 presets, lengths log-uniform 5-300 s",
+           "bank_gb": float(bank.nbytes) / 1e9,
+           "config": {"workload": ("requests over 8 presets of the HBM-bank kind" if args.serve_bank == "large" else
+                                   "requests of the small kind over 8 presets") + ", lengths log-uniform 5-300 s",
                       "batch_jobs": args.serve_batch, "lanes": args.serve_lanes,
                       "publication": "as batches finish (cs_poll)",
                       "admission": "a batch launches while others run only if its estimated footprint fits in "

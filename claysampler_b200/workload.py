@@ -295,13 +295,17 @@ def write_uneven_batch(root: Path, seed: int = 3, jobs: int = 1024, presets: int
 
 
 def write_serving_jobs(root: Path, seed: int = 5, jobs: int = 200, presets: int = 8, low: float = 5.0,
-                       high: float = 300.0, rate: float = 50.0) -> tuple[list[Job], np.ndarray]:
+                       high: float = 300.0, rate: float = 50.0, large: bool = False) -> tuple[list[Job], np.ndarray]:
     """Render requests of the serving kind: jobs over several presets of the small
-    kind, MIDI lengths log-uniform in [low, high] seconds at the small kind's note
-    density, arriving by a Poisson process of `rate` jobs per second.  Returns the
-    jobs and their arrival times in seconds."""
+    kind (`large`: of the HBM-bank kind, about 1.5 GB of float samples each), MIDI
+    lengths log-uniform in [low, high] seconds at the small kind's note density,
+    arriving by a Poisson process of `rate` jobs per second.  Returns the jobs and
+    their arrival times in seconds."""
     root.mkdir(parents=True, exist_ok=True)
-    sfzs = [write_plain_small_preset(root, seed + p, name=f"serve{p}") for p in range(presets)]
+    if large:
+        sfzs = [write_hbm_preset(root, seed + p, name=f"serve_large{p}") for p in range(presets)]
+    else:
+        sfzs = [write_plain_small_preset(root, seed + p, name=f"serve{p}") for p in range(presets)]
     rng = np.random.default_rng(seed + 2000)
     lengths = np.exp(rng.uniform(np.log(low), np.log(high), jobs))
     arrivals = np.cumsum(rng.exponential(1.0 / rate, jobs))
