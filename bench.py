@@ -163,17 +163,58 @@ def plan_jobs(jobs):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed region:
+    NVML read every 2 ms from a thread (read-only queries), else nvidia-smi."""
     FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.nvml = None
         self.lines = []
+        self.samples = []               # (sm MHz, max MHz, reasons) from NVML
+        self.stop = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _nvml_sample(self):
+        pynvml, handle = self.nvml
+        sm = pynvml.nvmlDeviceGetClockInfo(handle, pynvml.NVML_CLOCK_SM)
+        top = pynvml.nvmlDeviceGetMaxClockInfo(handle, pynvml.NVML_CLOCK_SM)
+        bits = pynvml.nvmlDeviceGetCurrentClocksEventReasons(handle)
+        flags = (pynvml.nvmlClocksEventReasonHwSlowdown, pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                 pynvml.nvmlClocksEventReasonSwThermalSlowdown, pynvml.nvmlClocksEventReasonSwPowerCap)
+        self.samples.append((float(sm), float(top), {n for n, f in zip(self.NAMES, flags) if bits & f}))
+
+    def _nvml_loop(self):
+        while not self.stop.is_set():
+            try:
+                self._nvml_sample()
+            except Exception:
+                return
+            time.sleep(0.002)
 
     def __enter__(self):
+        try:
+            self.nvml = self._nvml_handle()
+            self._nvml_sample()
+            self.samples.clear()
+            self.thread = threading.Thread(target=self._nvml_loop, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                                           "-lms", "50", "-i", str(self.index)],
@@ -195,6 +236,14 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *exc):
+        if self.nvml:
+            self.stop.set()
+            self.thread.join(timeout=1)
+            if not self.samples:        # a region shorter than one period: read once at its end
+                try:
+                    self._nvml_sample()
+                except Exception:
+                    pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -204,7 +253,10 @@ class ClockSampler:
 
     def summary(self):
         sm, top, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for clock, peak, active in self.samples:
+            sm.append(clock)
+            top = max(top, peak)
+            reasons |= active
         for line in self.lines:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 7:
@@ -214,11 +266,12 @@ class ClockSampler:
                 top = max(top, float(parts[1]))
             except ValueError:
                 continue
-            for name, flag in zip(names, parts[3:7]):
+            for name, flag in zip(self.NAMES, parts[3:7]):
                 if flag.lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": top or None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvml" if self.nvml else "nvidia-smi"}
 
 
 def gather_rows(totals, world):
@@ -660,7 +713,7 @@ def serving_requests(args, rank):
     and sample bank."""
     from claysampler_b200 import workload as wl
     from claysampler_b200.host import Host
-    large = args.serve_bank == "large"
+    large = getattr(args, "serve_bank", "small") == "large"
     root = args.workdir / f"serving_s{args.seed + rank}_j{args.serve_jobs}_r{args.serve_rate:g}{'_large' if large else ''}"
     marker = root / "ready"
     if not marker.exists():
@@ -725,7 +778,8 @@ def run_serve(args):
            "wall_s": wall, "n_gpus": 1, "dtype": "f32", "data": "synthetic (seeded SFZ/WAV/MIDI)",
            "deferred_launches": renderer.deferred_launches,
            "bank_gb": float(bank.nbytes) / 1e9,
-           "config": {"workload": ("requests over 8 presets of the HBM-bank kind" if args.serve_bank == "large" else
+           "config": {"workload": ("requests over 8 presets of the HBM-bank kind"
+                                   if getattr(args, "serve_bank", "small") == "large" else
                                    "requests of the small kind over 8 presets") + ", lengths log-uniform 5-300 s",
                       "batch_jobs": args.serve_batch, "lanes": args.serve_lanes,
                       "publication": "as batches finish (cs_poll)",
