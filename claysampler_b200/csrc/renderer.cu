@@ -23,6 +23,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <deque>
+#include <future>
 #include <limits>
 #include <memory>
 #include <tuple>
@@ -912,7 +913,10 @@ struct cs_renderer {
     size_t bankCapacity = 0, uploaded = 0;
     size_t scratchLimit = 0;            // 0: derive from free memory
     bool sharedSources = true;          // render each shared voice source once per batch
-    size_t budgetCache = 0;             // derived scratch budget of the current render call (0: stale)
+    // Derived scratch budget (0: read it again).  cudaMemGetInfo can take
+    // milliseconds while other work runs, so it is read once and kept until the
+    // bank is uploaded or a batch arena does not fit.
+    size_t budgetCache = 0;
     size_t deferred = 0;                // serving: launches deferred for lack of free memory
     // Largest staging, download and arena sizes any lane has needed (lanes grow to them).
     size_t stagingHigh = 0, downloadHigh = 0, arenaHigh = 0;
@@ -1042,7 +1046,7 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
             p->groups.push_back(make_int2(int(first), int(end)));
         }
     }
-    // The derived budget is read once per render call (cudaMemGetInfo is slow).
+    // The derived budget is read once and kept (cudaMemGetInfo is slow).
     if (!r.scratchLimit && !r.budgetCache)
         r.budgetCache = defaultScratchBudget();
     size_t scratchBudget = r.scratchLimit ? r.scratchLimit : r.budgetCache;
@@ -1566,19 +1570,30 @@ public:
 
     void render(const cs_plan* plans, size_t count)
     {
-        r.budgetCache = 0;
         r.oomBudget = 0;
         queue.assign(plans, plans + count);
         next = 0;
         // One shared-source pool for the whole window (volume groups render
-        // their chunks apart, so they keep per-batch sources).
+        // their chunks apart, so they keep per-batch sources).  A worker thread
+        // plans it while the first batch is staged with sources of its own; the
+        // pool serves the batches from the second on.
         WindowSources window;
         struct Detach {
-            cs_renderer& r;
-            ~Detach() { r.window = nullptr; }
-        } detach{r};
-        r.window = r.sharedSources && r.orderedCompute && r.groupMinimum <= 0 && poolWindow(window, plans, count)
-            ? &window : nullptr;
+            WindowRenderer& w;
+            ~Detach()
+            {
+                if (w.windowPlan.valid())
+                    w.windowPlan.wait();
+                w.r.window = nullptr;
+                w.pendingWindow = nullptr;
+            }
+        } detach{*this};
+        r.window = nullptr;
+        pendingWindow = nullptr;
+        if (r.sharedSources && r.orderedCompute && r.groupMinimum <= 0) {
+            pendingWindow = &window;
+            windowPlan = std::async(std::launch::async, [&window, plans, count] { return window.plan(plans, count); });
+        }
         for (;;) {
             launch(true);
             if (flight.empty())
@@ -1589,11 +1604,24 @@ public:
         std::fprintf(stderr, "SCHEDULE\tjobs=%zu\trounds=%zu\trefills=%zu\n", queue.size(), rounds, refills);
     }
 
-    // Plans the window's shared sources and places their pool, within half the
-    // scratch budget; false when nothing is shared or the pool does not fit.
-    bool poolWindow(WindowSources& window, const cs_plan* plans, size_t count)
+    // The window planned on the worker thread, attached once a batch is in flight.
+    WindowSources* pendingWindow = nullptr;
+    std::future<size_t> windowPlan;
+
+    void attachWindow()
     {
-        const size_t floats = window.plan(plans, count);
+        if (!pendingWindow || flight.empty())
+            return;
+        WindowSources& window = *pendingWindow;
+        pendingWindow = nullptr;
+        const size_t floats = windowPlan.get();
+        r.window = poolWindow(window, floats) ? &window : nullptr;
+    }
+
+    // Places the pool of a planned window (`floats` floats), within half the
+    // scratch budget; false when nothing is shared or the pool does not fit.
+    bool poolWindow(WindowSources& window, size_t floats)
+    {
         if (!floats)
             return false;
         if (!r.scratchLimit && !r.budgetCache)
@@ -1625,7 +1653,6 @@ public:
     size_t submit(const cs_plan* plans, size_t count)
     {
         const size_t ticket = ticketBase + queue.size();
-        r.budgetCache = 0;
         r.oomBudget = 0;
         queue.insert(queue.end(), plans, plans + count);
         launch(false, true);
@@ -1740,6 +1767,7 @@ private:
                 next = renderAlone(next, jobs);
                 continue;
             }
+            attachWindow();
             const int lane = freeLane();
             cs_prepared* prepared = tryPrepare(next, jobs, lane);
             if (!prepared) {
@@ -2321,6 +2349,7 @@ int cs_upload_samples(cs_renderer* r, const float* pcm, size_t floats, int fresh
         if (!r)
             throw std::runtime_error("null renderer");
         cs::check(cudaSetDevice(r->device), "CUDA device");
+        r->budgetCache = 0;
         if (fresh)
             r->uploaded = 0;
         if (floats <= r->uploaded && r->bank)
