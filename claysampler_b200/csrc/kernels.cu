@@ -942,8 +942,13 @@ constexpr int kMixStaged = kMixThreads / kTilesPerBlock;     // staged voices pe
 // staged gains instead of walking bindings and evaluating pan gains, and looks up
 // no track point where the tile sits on one line of each track.  Every value is
 // the one the per-frame expressions give, so the sums are unchanged.
-template <bool Natural, int Inline>
-__global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(BatchView b, SegmentView s, StereoStats* stats)
+// Part 0 mixes any block; Part 1 mixes only blocks of unmodulated shared-source
+// voices (the four-frame path) and appends the others to `deferred` (a count,
+// then block indices); Part 2 mixes a deferred block.  Splitting keeps the lean
+// pass free of the general path's registers.
+template <bool Natural, int Inline, int Part>
+__device__ __forceinline__ void mixBlock(const BatchView& b, const SegmentView& s, StereoStats* stats, int block,
+                                         int* deferred)
 {
     __shared__ double reduceD[32];
     __shared__ float reduceF[32];
@@ -955,7 +960,6 @@ __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(Ba
     // Per warp: bit k of mixed / general marks tile k as not all staged stereo
     // filtered voices / not all staged kind 5 / 6 voices.
     __shared__ unsigned warpFlags[kMixThreads / 32][2];
-    const int block = s.blocks[blockIdx.x];
     const int jobIndex = b.blockJob[block];
     const JobInfo job = b.jobs[jobIndex];
     const int local = block - job.blockFirst;
@@ -1014,6 +1018,11 @@ __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(Ba
         mixedTiles |= warpFlags[w][0];
         generalTiles |= warpFlags[w][1];
     }
+    if (Part == 1 && generalTiles != 0) {
+        if (threadIdx.x == 0)
+            deferred[1 + atomicAdd(deferred, 1)] = block;
+        return;
+    }
     double power = 0;
     float peak = 0;
     if (Inline == 2 && generalTiles == 0) {
@@ -1070,7 +1079,7 @@ __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(Ba
                 static_cast<short2*>(b.mix)[job.offset + frame] = make_short2(toPcm16(x), toPcm16(y));
             }
         }
-    } else
+    } else if (Part != 1)
     for (int k = 0; k < kTilesPerBlock; ++k) {
         const int frame = local * kBlockFrames + k * kTileFrames + int(threadIdx.x);
         if (frame >= job.frames || frame < s.first || frame >= s.end)
@@ -1194,6 +1203,31 @@ __global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(Ba
         blockStats(power, peak, reduceD, reduceF);
         if (threadIdx.x == 0)
             stats[block] = {power, peak};
+    }
+}
+
+template <bool Natural, int Inline>
+__global__ void __launch_bounds__(kMixThreads, Inline == 1 ? 5 : 8) mixKernel(BatchView b, SegmentView s, StereoStats* stats)
+{
+    mixBlock<Natural, Inline, 0>(b, s, stats, s.blocks[blockIdx.x], nullptr);
+}
+
+template <bool Natural>
+__global__ void __launch_bounds__(kMixThreads, 8) mixLeanKernel(BatchView b, SegmentView s, StereoStats* stats,
+                                                                 int* deferred)
+{
+    mixBlock<Natural, 2, 1>(b, s, stats, s.blocks[blockIdx.x], deferred);
+}
+
+// The deferred blocks, each CTA taking every gridDim.x-th.
+template <bool Natural>
+__global__ void __launch_bounds__(kMixThreads, 8) mixDeferredKernel(BatchView b, SegmentView s, StereoStats* stats,
+                                                                     const int* deferred)
+{
+    const int count = deferred[0];
+    for (int i = int(blockIdx.x); i < count; i += int(gridDim.x)) {
+        mixBlock<Natural, 2, 2>(b, s, stats, deferred[1 + i], nullptr);
+        __syncthreads();                // the next block restages the shared arrays
     }
 }
 
@@ -1866,10 +1900,11 @@ void launchTileIndex(const BatchView& b, const JobSpans* spans, const int2* unit
         tileIndexKernel<<<unitCount, kIndexThreads, 0, stream>>>(b, spans, units, tiles, indices);
 }
 
-void launchMix(const BatchView& b, const SegmentView& s, bool natural, StereoStats* stats, cudaStream_t stream)
+int launchMix(const BatchView& b, const SegmentView& s, bool natural, StereoStats* stats, int* deferred,
+              cudaStream_t stream)
 {
     if (!s.blockCount)
-        return;
+        return 0;
     if (b.inlineVoices == 1)
         setOncePerDevice(2, [] {
             return firstError({cudaFuncSetAttribute(mixKernel<true, 1>, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -1883,11 +1918,32 @@ void launchMix(const BatchView& b, const SegmentView& s, bool natural, StereoSta
             launch(mixKernel<true, 1>);
         else
             launch(mixKernel<false, 1>);
-    } else if (natural) {
-        launch(mixKernel<true, 2>);
-    } else {
-        launch(mixKernel<false, 2>);
+        return 1;
     }
+    if (!b.sharedRefs) {
+        // No shared sources: every voice is filtered.
+        if (natural)
+            launch(mixKernel<true, 2>);
+        else
+            launch(mixKernel<false, 2>);
+        return 1;
+    }
+    {
+        // The lean pass over every block, then the blocks it deferred.
+        int device = 0, sms = 0;
+        cudaGetDevice(&device);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        const int grid = std::max(1, std::min(s.blockCount, std::max(sms, 1) * 8));
+        cudaMemsetAsync(deferred, 0, sizeof(int), stream);
+        if (natural) {
+            mixLeanKernel<true><<<s.blockCount, kMixThreads, 0, stream>>>(b, s, stats, deferred);
+            mixDeferredKernel<true><<<grid, kMixThreads, 0, stream>>>(b, s, stats, deferred);
+        } else {
+            mixLeanKernel<false><<<s.blockCount, kMixThreads, 0, stream>>>(b, s, stats, deferred);
+            mixDeferredKernel<false><<<grid, kMixThreads, 0, stream>>>(b, s, stats, deferred);
+        }
+    }
+    return 2;
 }
 
 int launchFinish(const BatchView& b, const FinishView& f, bool natural, bool quality, const TailConfig& tail,

@@ -226,7 +226,11 @@ int launchSharedSources(const BatchView& b, const SharedSource* sources, const i
 int launchSources(const BatchView& b, const SegmentView& s, cudaStream_t stream);
 int launchRecurrences(const BatchView& b, const SegmentView& s, cudaStream_t stream);
 int launchGeneralChains(const BatchView& b, const SegmentView& s, cudaStream_t stream);
-void launchMix(const BatchView& b, const SegmentView& s, bool natural, StereoStats* stats, cudaStream_t stream);
+// `deferred`: device scratch of 1 + blocks ints for the blocks the lean mix pass
+// leaves to the general one.
+// Returns the kernels launched.
+int launchMix(const BatchView& b, const SegmentView& s, bool natural, StereoStats* stats, int* deferred,
+              cudaStream_t stream);
 int launchFinish(const BatchView& b, const FinishView& f, bool natural, bool quality, const TailConfig& tail,
                  cudaStream_t stream);
 // Onset levels (quality gate only) and per-job verdicts on the finished PCM.

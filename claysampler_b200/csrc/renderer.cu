@@ -844,6 +844,7 @@ struct cs_prepared {
     std::vector<cs::SegmentView> segments;
     cs::FinishView finish{};
     cs::StereoStats* stereo = nullptr;
+    int* deferredBlocks = nullptr;      // the mix's lean pass defers blocks here
     size_t stateBytes = 0, resultBytes = 0, mixBytes = 0;
     bool natural = true;
     int launches = 0;
@@ -1104,6 +1105,7 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     p->mixBytes = batch.frames * frameBytes;
     const size_t oMix = section(p->mixBytes);
     const size_t oStereo = section(size_t(batch.blocks) * sizeof(StereoStats));
+    const size_t oDeferred = section((size_t(batch.blocks) + 1) * sizeof(int));
     const size_t oWindows = section(size_t(batch.windows) * sizeof(MonoStats));
     const size_t oMono = section(r.natural ? batch.frames * sizeof(short) : 0);
     const size_t oPacked = section(batch.frames * size_t(channels) * sizeof(short));
@@ -1336,6 +1338,7 @@ cs_prepared* prepare(cs_renderer& r, const cs_plan* plans, size_t count, bool sh
     f.blockCount = batch.blocks;
     f.windowCount = batch.windows;
     p->stereo = f.stereo;
+    p->deferredBlocks = reinterpret_cast<int*>(base + oDeferred);
     p->output = f.packed;
     if (assess) {
         f.bodyPower = reinterpret_cast<unsigned long long*>(base + oBodyPower);
@@ -1450,8 +1453,7 @@ void run(cs_renderer& r, cs_prepared& p, cudaStream_t stream)
         stage(2);
         launches += launchGeneralChains(view, s, stream);
         stage(3);
-        launchMix(view, s, r.natural, p.stereo, stream);
-        launches += s.blockCount > 0;
+        launches += launchMix(view, s, r.natural, p.stereo, p.deferredBlocks, stream);
         stage(4);
     }
     check(cudaGetLastError(), "CUDA synthesis launch");
