@@ -1544,7 +1544,7 @@ __device__ __noinline__ short fadeSample(short value, int index, int count)
 // totals in any order.  A warp per 1024-frame block (eight per CTA), each lane
 // every 32nd frame; the reductions are warp shuffles, so no CTA barrier is needed.
 template <int Channels, bool Assess>
-__global__ void __launch_bounds__(kFinalizeWarps * 32, Assess ? 4 : 6) finalizeKernel(BatchView b, FinishView f, const short* input,
+__global__ void __launch_bounds__(kFinalizeWarps * 32, 4) finalizeKernel(BatchView b, FinishView f, const short* input,
                                                                       int quality)
 {
     const int block = int(blockIdx.x) * kFinalizeWarps + int(threadIdx.x >> 5);
@@ -1579,8 +1579,11 @@ __global__ void __launch_bounds__(kFinalizeWarps * 32, Assess ? 4 : 6) finalizeK
     const int fadeStart = frames - fade;
     const short* __restrict__ source = input + job.offset * Channels;
     short* __restrict__ packed = f.packed + outputOffset * Channels;
-    // Each lane takes kUnroll frames 32 apart per step, their loads issued together.
-    constexpr int kUnroll = 4;
+    // Each lane takes kUnroll frames 32 apart per step, their loads issued together:
+    // sixteen 2-byte loads in flight per lane (four CTAs per SM) keep enough bytes
+    // in flight to hide DRAM latency, which four did not (0.935 against 0.975 ms on
+    // a 293 M-frame batch).
+    constexpr int kUnroll = 16;
     for (int base = first + lane; base < end; base += 32 * kUnroll) {
         short loaded[kUnroll][Channels];
         #pragma unroll
