@@ -964,8 +964,13 @@ __device__ __forceinline__ void mixBlock(const BatchView& b, const SegmentView& 
     const JobInfo job = b.jobs[jobIndex];
     const int local = block - job.blockFirst;
     const int jobTiles = (job.frames + kTileFrames - 1) / kTileFrames;
-    if (threadIdx.x < kTilesPerBlock * 3) {
-        const int k = int(threadIdx.x) / 3, track = int(threadIdx.x) % 3;
+    // Tile k's three tracks are staged by threads 32-34 of its group of kMixStaged
+    // threads: a warp whose first lanes stage voices (a tile rarely holds more than
+    // 32), so the track lookups and the voice staging run in different warps instead
+    // of one after the other in the same one.
+    static_assert(kMixStaged == 64 && kTilesPerBlock * kMixStaged == kMixThreads, "one 64-thread group per tile");
+    if ((threadIdx.x & 63) >= 32 && (threadIdx.x & 63) < 35) {
+        const int k = int(threadIdx.x) >> 6, track = int(threadIdx.x & 63) - 32;
         const int first = local * kBlockFrames + k * kTileFrames;
         const int last = min(first + kTileFrames, max(job.frames, first + 1)) - 1;
         tracks[k][track] = tileTrackOf(b.points, job.tracks[track], job.tracks[track + 1], first, last);
@@ -981,14 +986,15 @@ __device__ __forceinline__ void mixBlock(const BatchView& b, const SegmentView& 
                 mixed = general = 1u << k;
         }
         if (i < tile.count && tile.count <= kMixStaged) {
+            const int first = local * kBlockFrames + k * kTileFrames;
+            // The tile's pan track, as the track staging above finds it; looked up
+            // before the voice so that its loads and the voice's overlap.
+            const TileTrack pan = tileTrackOf(b.points, job.tracks[2], job.tracks[3], first,
+                                              min(first + kTileFrames, max(job.frames, first + 1)) - 1);
             MixVoice m = mixVoiceOf(b, s, __ldg(b.indices + tile.first + i));
             if (m.kind != 1)
                 mixed |= 1u << k;
-            const int first = local * kBlockFrames + k * kTileFrames;
             if (m.kind >= 3) {
-                // The tile's pan track, as the track staging above finds it.
-                const TileTrack pan = tileTrackOf(b.points, job.tracks[2], job.tracks[3], first,
-                                                  min(first + kTileFrames, max(job.frames, first + 1)) - 1);
                 const cs_voice_span& v = b.voices[m.index];
                 if (v.modulationCount == 0 && !v.stereoMatrix && tileTrackFixed(pan, first)) {
                     // voiceOutputFrom with no bindings: the pan offset is the track's.
