@@ -1,7 +1,11 @@
 """Autotuner for the end-to-end render (render_window through the C ABI).
 
 The tap count is fixed at 48 and tiles are 256 frames because the tail blocks
-are 1024 frames, so neither is a free parameter.  What does change the
+are 1024 frames, so neither is a free parameter.  Frames per segment are not
+swept either: the renderer cuts a batch into the longest segments its chain
+scratch budget holds (one segment unless filtered voices' storage exceeds it),
+and shorter segments only add launches and state carries; batches of unfiltered
+voices have no chain scratch to cut.  What does change the
 end-to-end rate without changing a sample is how the work is cut and overlapped:
 
 * `batch_jobs` (the CLI's --gpu-batch-jobs): how many jobs one GPU batch takes.
