@@ -56,12 +56,12 @@ sys.path.insert(0, str(ROOT))
 
 RATE = 44100
 METRIC = "audio-sec/sec on 1 B200 (batched+learned vs plain, ≤1 LSB); HBM GB/s; p99"
-WORKLOAD = "plain batch: 64 jobs, 88 keys x 4 layers stereo 24-bit, lpf_2p + fileg + 5 Hz LFO, loops, pedal"
+WORKLOAD = "plain batch: {jobs} jobs, 88 keys x 4 layers stereo 24-bit, lpf_2p + fileg + 5 Hz LFO, loops, pedal"
 WORKLOADS = {
     "plain_batch": WORKLOAD,
-    "uneven": "uneven batch: 1024 jobs over 4 presets of 12 mono 16-bit regions (48-tap sinc resampling, "
+    "uneven": "uneven batch: {jobs} jobs over 4 presets of 12 mono 16-bit regions (48-tap sinc resampling, "
               "no filter), Pareto(1.5) lengths 2-600 s",
-    "uneven_hbm": "uneven batch with an HBM-resident bank: 1024 jobs over 4 presets of 22 keycenters x 8 "
+    "uneven_hbm": "uneven batch with an HBM-resident bank: {jobs} jobs over 4 presets of 22 keycenters x 8 "
                   "velocity layers x 48 s mono (about 6 GB of float samples), Pareto(1.5) lengths 2-600 s",
 }
 # Jobs of the bounded CPU sample (the reference arm's step and the cpu_baseline /
@@ -367,7 +367,7 @@ def sample_jobs(args):
 
 def bench_config(args, jobs, ranks):
     """The `config` object of the bench line, identical in both arms."""
-    return {"workload": WORKLOADS[args.workload], "jobs_per_gpu": len(jobs), "seed": args.seed, "tail": "natural",
+    return {"workload": WORKLOADS[args.workload].format(jobs=len(jobs)), "jobs_per_gpu": len(jobs), "seed": args.seed, "tail": "natural",
             "taps": 48, "l2": "each step writes a float mix above the 126 MB L2, evicting it (no flush)",
             "parallelism": f"jobs sharded by rank, {ranks} rank(s)"}
 
